@@ -99,6 +99,9 @@ def test_oracle_matches_committed_reference_outputs():
             assert y[int(i)] == complex(float.fromhex(re_), float.fromhex(im_))
 
 
+PI_L = np.arccos(np.longdouble(-1))
+
+
 def _kind1(N):
     # input.c:218-224 and its closed form :260-266 (theta = 1)
     j = np.arange(N, dtype=np.longdouble)
@@ -106,7 +109,7 @@ def _kind1(N):
     k = np.arange(N, dtype=np.longdouble)
     arg = np.longdouble(N)
     num = 1 - np.cos(arg) - 1j * np.sin(arg)
-    ang = 1 - 2 * np.pi * k / N
+    ang = 1 - 2 * PI_L * k / N
     s = np.sin(ang / 2)
     den = 2 * s * s - 1j * np.sin(ang)
     return x, (num / den).astype(np.complex128)
@@ -122,9 +125,9 @@ def _kind0(N):
     L = np.floor(A + 0.5)
     f = (k * W - L * N) / N
     sgn = np.where(L.astype(np.int64) & 1, -1.0, 1.0)
-    den = np.where(2 * k <= N, W * np.sin(np.pi * k / N), W * np.sin(np.pi * (N - k) / N))
+    den = np.where(2 * k <= N, W * np.sin(PI_L * k / N), W * np.sin(PI_L * (N - k) / N))
     with np.errstate(divide="ignore", invalid="ignore"):
-        X = sgn * np.sin(np.pi * f) / den
+        X = sgn * np.sin(PI_L * f) / den
     X[0] = 1
     return x, X.astype(np.complex128)
 

@@ -1,0 +1,163 @@
+/*
+ * soi_b200.h -- C ABI of the B200 (sm_100a) SOI FFT library, libsoi_b200.so.
+ *
+ * Drop-in for the reference's public API, soi.h:236-280 (IntelLabs/SOI_FFT):
+ * the same descriptor field names and the same four entry points, plus
+ * status-returning variants and device-level entry points.  Plain C types
+ * only: pointers, sizes, ints, doubles.
+ *
+ * Differences a caller of the reference must know:
+ *   - One process, one GPU.  P (MPI ranks) must be 1 and rank 0; the segment
+ *     count is S = k (the reference's S = k*P).  `comm` stands in for
+ *     MPI_Comm and is not used.
+ *   - alpha_dt holds N complex inputs and receives N complex outputs in
+ *     natural DFT order (the reference's rank r holds N/P inputs and gets
+ *     segments [segmentBoundaries[r], segmentBoundaries[r+1]) * M outputs).
+ *   - precision selects the element type of alpha_dt:
+ *       SOI_PRECISION_FP64       double complex (cfft_complex_t, soi.h:227)
+ *       SOI_PRECISION_SPLIT_FP32 float complex (complex64 storage)
+ *   - device_ptr = 0: alpha_dt is host memory, copied in and out inside
+ *     compute_soi.  device_ptr = 1: alpha_dt is device memory.
+ *   - The void entry points print a message and exit(-1) on an unsupported
+ *     configuration, as the reference does (pfft.c:157-183,
+ *     parallel_filter_subsampling.cpp:89-94,543-548).  The *_status
+ *     variants return a soi_status_t instead.
+ */
+#ifndef SOI_B200_H
+#define SOI_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef size_t cfft_size_t;        /* soi.h:220 */
+typedef void *soi_comm_t;          /* stands in for MPI_Comm (soi.h:238) */
+
+typedef enum {
+  SOI_PRECISION_FP64 = 0,          /* plain method, FP64 complex throughout        */
+  SOI_PRECISION_SPLIT_FP32 = 1     /* complex64 storage, FP32 arithmetic,
+                                      FP64-generated tables rounded once          */
+} soi_precision_t;
+
+typedef enum {
+  SOI_OK = 0,
+  SOI_ERR_INVALID = 1,             /* bad sizes / parameters                      */
+  SOI_ERR_UNSUPPORTED = 2,         /* valid for the reference, not built here     */
+  SOI_ERR_CUDA = 3,                /* a CUDA runtime call failed                  */
+  SOI_ERR_NOT_INITIALISED = 4,
+  SOI_ERR_TIMEOUT = 5              /* a bounded device-side wait gave up          */
+} soi_status_t;
+
+/* Descriptor.  Field names follow soi_desc_t, soi.h:236-270. */
+typedef struct {
+  soi_comm_t comm;        /* soi.h:238, unused                                   */
+  int P;                  /* soi.h:239, must be 1                                */
+  int rank;               /* soi.h:240, must be 0                                */
+  cfft_size_t k;          /* soi.h:241, segments (S = k*P)                       */
+  cfft_size_t N;          /* soi.h:242, transform length                         */
+  int n_mu;               /* soi.h:252, oversampling numerator                   */
+  int d_mu;               /* soi.h:253, oversampling denominator                 */
+  cfft_size_t B;          /* soi.h:254, window taps                              */
+  double tau;             /* soi.h:255                                           */
+  double sigma;           /* soi.h:256                                           */
+  int use_vlc;            /* soi.h:266, VLC round trip of the transposed data    */
+  int *segmentBoundaries; /* soi.h:267, [0, S] after init                        */
+  double comm_to_comp_cost_ratio; /* soi.h:269, kept for source compatibility    */
+  /* additions */
+  int precision;          /* soi_precision_t                                     */
+  int device_ptr;         /* alpha_dt is a device pointer                        */
+  int device;             /* CUDA device ordinal                                 */
+  void *stream;           /* cudaStream_t to run on (NULL: the library's own)    */
+  int last_status;        /* soi_status_t of the last call                       */
+  void *plan;             /* opaque device state                                 */
+} soi_desc_t;
+
+/* ---- reference entry points (soi.h:272-280) --------------------------- */
+
+/* pfft.c:84-138: n_mu=5, d_mu=4, tau=928/1024, sigma=373.7314, B=72,
+ * use_vlc=0, plus P=1, rank=0, precision=FP64, device_ptr=0, device=0. */
+void set_default_soi_descriptor(soi_desc_t *desc);
+
+/* pfft.c:140-232: tabulates the windows and sets up the device plan. */
+void init_soi_descriptor(soi_desc_t *desc, soi_comm_t comm, cfft_size_t k);
+
+/* pfft.c:276-721: in-place transform of alpha_dt (see precision, device_ptr). */
+void compute_soi(soi_desc_t *desc, void *alpha_dt);
+
+/* pfft.c:234-267 */
+void free_soi_descriptor(soi_desc_t *desc);
+
+/* parallel_filter_subsampling.cpp:535-550: stage 1 only (convolution, S-point
+ * FFTs and segment transpose) into the descriptor's device buffer; fetch it
+ * with soi_get_transposed. */
+void parallel_filter_subsampling(soi_desc_t *desc, void *alpha_dt);
+
+/* ---- status-returning variants ---------------------------------------- */
+int soi_init_status(soi_desc_t *desc, soi_comm_t comm, cfft_size_t k);
+int soi_compute_status(soi_desc_t *desc, void *alpha_dt);
+int soi_filter_subsampling_status(soi_desc_t *desc, void *alpha_dt);
+int soi_free_status(soi_desc_t *desc);
+const char *soi_status_string(int status);
+
+/* Copy the transposed data (alpha_tilde of the reference: S segments of
+ * M' = n_mu*M/d_mu elements, segment-major) to dst (host or device per
+ * desc->device_ptr), element type per desc->precision. */
+int soi_get_transposed(soi_desc_t *desc, void *dst);
+
+/* ---- device-level entry points (device pointers, desc->stream) --------- */
+
+/* Stage 1 from a device input to a device transposed buffer (S x M'). */
+int soi_filter_subsample_device(soi_desc_t *desc, const void *alpha_dev, void *transposed_dev);
+/* Stage 2: M'-point FFT of each segment, demodulation, discard; reads and
+ * overwrites transposed_dev, writes N outputs to out_dev. */
+int soi_segment_fft_demod_device(soi_desc_t *desc, void *transposed_dev, void *out_dev);
+
+/* Plan geometry without touching a GPU (host logic, for tests and tuning):
+ * info[0..15] = S, M, M', stage-1 groups per tile JT, taps per phase,
+ * groups per thread JR, stage-1 shared bytes, M1, M2, C1, C2, pass-1 and
+ * pass-2 shared bytes, radix stages of the S-, M1- and M2-point FFTs. */
+int soi_plan_geometry(const soi_desc_t *desc, cfft_size_t k, long long *info);
+
+/* Kernel timings of the last compute (milliseconds, CUDA events on the
+ * launching stream): [0] stage 1, [1] stage 2, [2] VLC, [3] whole compute. */
+int soi_last_timings(soi_desc_t *desc, float *ms4);
+/* Enable/disable event timing (off by default). */
+int soi_set_timing(soi_desc_t *desc, int enable);
+
+/* ---- VLC (compress.c) on the device ------------------------------------ */
+
+/* compress.c:11-131 over nchunks chunks of `len` doubles each (device
+ * pointers): e_max_out[c] = max biased exponent of chunk c minus 1023. */
+int soi_vlc_max_exponent_device(const double *x_dev, int len, int nchunks,
+                                int *e_max_out_dev, void *stream);
+/* compress.c:205-372 for each chunk: words_dev + c*stride_words receives the
+ * compressed words, nwords_dev[c] their count.  e_max is the global maximum
+ * exponent, e_max_i_dev[c] the chunk's.  len must be a multiple of 16. */
+int soi_vlc_compress_device(const double *x_dev, int len, int nchunks, int e_max,
+                            const int *e_max_i_dev, int *words_dev, long stride_words,
+                            int *nwords_dev, void *stream);
+/* compress.c:428-544 for each chunk (len a multiple of 16). */
+int soi_vlc_decompress_device(const int *words_dev, long stride_words, int len, int nchunks,
+                              int e_max, const int *e_max_i_dev, double *out_dev, void *stream);
+/* Words compress() writes for one chunk (pfft.c:397-402 sizing). */
+int soi_vlc_words(int len, int e_max, int e_max_i);
+
+/* ---- host-side tables (no GPU needed) ---------------------------------- */
+
+/* The factorised window the kernels use: for output phase theta, tap kk and
+ * column s the reference's w[theta][kk][s] (pfft.c:42-66) equals
+ * phase[theta][s] * filt[kk][theta][s], with filt real.  filt: B*n_mu*S
+ * doubles ([kk][theta][s]), phase: n_mu*S complex ([theta][s]),
+ * W_inv: N/S complex (pfft.c:68-82).  Any pointer may be NULL. */
+int soi_window_tables(cfft_size_t N, cfft_size_t S, int n_mu, int d_mu, cfft_size_t B,
+                      double tau, double sigma, double *filt, double *phase, double *W_inv);
+
+/* Library version string. */
+const char *soi_b200_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

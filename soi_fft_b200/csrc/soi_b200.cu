@@ -1,0 +1,709 @@
+// soi_b200.cu -- host side of libsoi_b200.so: the C ABI of include/soi_b200.h,
+// descriptor/plan lifecycle (pfft.c:84-267), long-double table generation
+// and the launches of the stage-1/stage-2 kernels (soi_kernels.cuh).
+#include <cuda_runtime.h>
+
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "../../include/soi_b200.h"
+#include "soi_kernels.cuh"
+#include "vlc_kernels.cuh"
+
+using namespace soi;
+
+namespace {
+
+const long double kPi = 3.141592653589793238462643383279502884197169399375L;
+
+struct Plan {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int prec = SOI_PRECISION_FP64;
+  size_t elem = 16;            // bytes per complex element
+  size_t N = 0, S = 0, M = 0, Mh = 0, J = 0, B = 0;
+  int nmu = 5, dmu = 4;
+  double tau = 0, sigma = 0;
+  int atap = 0, JR = 8, JT = 0, pitch = 0;
+  size_t smem1 = 0, smem_c = 0, smem_r = 0;
+  FftPlan planS{}, plan1{}, plan2{};
+  int M1 = 0, M2 = 0, C1 = 0, C2 = 0, lo_bits = 11;
+  void *d_filt = nullptr, *d_phase = nullptr, *d_twS = nullptr, *d_tw1 = nullptr, *d_tw2 = nullptr;
+  void *d_winv = nullptr, *d_wsmall = nullptr;
+  int *d_permS = nullptr, *d_perm1 = nullptr, *d_perm2 = nullptr;
+  double2 *d_xlo = nullptr, *d_xhi = nullptr;
+  void *d_T = nullptr;         // S*Mh complex
+  void *d_io = nullptr;        // N complex staging for host pointers
+  // VLC
+  double *d_vlc_x = nullptr;   // promoted/decompressed doubles (FP32 path)
+  int *d_vlc_words = nullptr, *d_vlc_n = nullptr, *d_vlc_emax = nullptr;
+  long vlc_stride = 0;
+  bool timing = false;
+  cudaEvent_t ev[5] = {};
+  float ms[4] = {0, 0, 0, 0};
+};
+
+#define CK(x)                                                                    \
+  do {                                                                           \
+    cudaError_t e__ = (x);                                                       \
+    if (e__ != cudaSuccess) {                                                    \
+      fprintf(stderr, "soi_b200: %s failed: %s\n", #x, cudaGetErrorString(e__)); \
+      return SOI_ERR_CUDA;                                                       \
+    }                                                                            \
+  } while (0)
+
+// ---- FFT planning ------------------------------------------------------------
+
+bool make_fft_plan(int L, FftPlan &p)
+{
+  memset(&p, 0, sizeof(p));
+  p.L = L;
+  int n = L, t = 0;
+  while (n % 8 == 0 && n > 8 && t < kMaxStages) { p.radix[t++] = 8; n /= 8; }
+  if (n == 8 && t < kMaxStages) { p.radix[t++] = 8; n = 1; }
+  while (n % 4 == 0 && t < kMaxStages) { p.radix[t++] = 4; n /= 4; }
+  while (n % 2 == 0 && t < kMaxStages) { p.radix[t++] = 2; n /= 2; }
+  while (n % 5 == 0 && t < kMaxStages) { p.radix[t++] = 5; n /= 5; }
+  while (n % 3 == 0 && t < kMaxStages) { p.radix[t++] = 3; n /= 3; }
+  while (n % 7 == 0 && t < kMaxStages) { p.radix[t++] = 7; n /= 7; }
+  p.nst = t;
+  return n == 1 && L >= 1;
+}
+
+// perm[k] = position of frequency k after the in-place DIF stages.
+std::vector<int> digit_reversal(const FftPlan &p)
+{
+  std::vector<int> perm(p.L);
+  for (int k = 0; k < p.L; ++k) {
+    int rem = k, span = p.L, pos = 0;
+    for (int s = 0; s < p.nst; ++s) {
+      span /= p.radix[s];
+      pos += (rem % p.radix[s]) * span;
+      rem /= p.radix[s];
+    }
+    perm[k] = pos;
+  }
+  return perm;
+}
+
+// ---- tables (long double, rounded once to the working precision) -----------
+
+// time window (pfft.c:42-66) factorised as phase * real filter:
+//   t = theta*d/n - kk - s/S + kappa/2, w = exp(i pi t) * y(t) / mu,
+//   exp(i pi t) = exp(i pi (theta*d/n + kappa/2 - s/S)) * (-1)^kk.
+long double window_y(long double t, double tau, double sigma)
+{
+  if (t == 0) return 1.0L;
+  long double a = kPi * (long double)tau * t;
+  return sinl(a) / a * expl(-kPi * kPi * t * t / (long double)sigma);
+}
+
+void host_tables(size_t N, size_t S, int n, int d, size_t B, double tau, double sigma, int atap,
+                 std::vector<long double> *filt, std::vector<long double> *ph_re,
+                 std::vector<long double> *ph_im, std::vector<long double> *wi_re,
+                 std::vector<long double> *wi_im)
+{
+  const long long kappa = (long long)B - d;
+  const long double mu = (long double)n / d;
+  const long long den = 2LL * n * (long long)S;  // t = num / den
+  size_t ntap = atap ? (size_t)atap * d : B;
+  if (filt) {
+    filt->assign(ntap * n * S, 0.0L);
+    for (size_t kk = 0; kk < B; ++kk)
+      for (int th = 0; th < n; ++th)
+        for (size_t s = 0; s < S; ++s) {
+          long long num = 2LL * th * d * (long long)S - 2LL * (long long)kk * n * (long long)S -
+                          2LL * (long long)s * n + kappa * n * (long long)S;
+          long double t = (long double)num / (long double)den;
+          long double y = window_y(t, tau, sigma) / mu;
+          (*filt)[(kk * n + th) * S + s] = (kk & 1) ? -y : y;
+        }
+  }
+  if (ph_re) {
+    ph_re->assign((size_t)n * S, 0);
+    ph_im->assign((size_t)n * S, 0);
+    const long long period = 2 * den;  // exp(i pi q/den) has period 2*den in q
+    for (int th = 0; th < n; ++th)
+      for (size_t s = 0; s < S; ++s) {
+        long long q = 2LL * th * d * (long long)S + kappa * n * (long long)S - 2LL * (long long)s * n;
+        q %= period;
+        if (q < 0) q += period;
+        long double ang = kPi * (long double)q / (long double)den;
+        (*ph_re)[th * S + s] = cosl(ang);
+        (*ph_im)[th * S + s] = sinl(ang);
+      }
+  }
+  if (wi_re) {
+    // pfft.c:68-82: W_inv[i] = exp(-i pi kappa i / M) / y_W(i/M - 1/2)
+    size_t M = N / S;
+    wi_re->assign(M, 0);
+    wi_im->assign(M, 0);
+    const long double sq = sqrtl((long double)sigma);
+    for (size_t i = 0; i < M; ++i) {
+      long double t = (long double)i / (long double)M - 0.5L;
+      long double y = (erfcl(sq * (t - tau / 2.0L)) - erfcl(sq * (t + tau / 2.0L))) / (2.0L * tau);
+      long long q = (long long)(((unsigned long long)kappa * i) % (2ULL * M));
+      long double ang = -kPi * (long double)q / (long double)M;
+      (*wi_re)[i] = cosl(ang) / y;
+      (*wi_im)[i] = sinl(ang) / y;
+    }
+  }
+}
+
+template <typename R>
+void round_complex(const std::vector<long double> &re, const std::vector<long double> &im, std::vector<R> &out)
+{
+  out.resize(2 * re.size());
+  for (size_t i = 0; i < re.size(); ++i) { out[2 * i] = (R)re[i]; out[2 * i + 1] = (R)im[i]; }
+}
+
+template <typename R>
+std::vector<R> roots_table(long long L)
+{
+  std::vector<R> t(2 * L);
+  for (long long m = 0; m < L; ++m) {
+    long double a = -2.0L * kPi * (long double)m / (long double)L;
+    t[2 * m] = (R)cosl(a);
+    t[2 * m + 1] = (R)sinl(a);
+  }
+  return t;
+}
+
+int upload(void **dst, const void *src, size_t bytes)
+{
+  CK(cudaMalloc(dst, bytes ? bytes : 16));
+  if (bytes) CK(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+  return SOI_OK;
+}
+
+// ---- kernel dispatch ---------------------------------------------------------
+
+template <typename R, int NMU, int JR>
+int launch_conv_t(Plan &p, const void *alpha, void *T, cudaStream_t st)
+{
+  ConvArgs a;
+  a.alpha = alpha; a.T = T; a.filt = p.d_filt; a.phase = p.d_phase; a.twS = p.d_twS;
+  a.permS = p.d_permS; a.wsmall = p.d_wsmall; a.planS = p.planS;
+  a.M = (long long)p.M; a.Mh = (long long)p.Mh; a.J = (long long)p.J;
+  a.S = (int)p.S; a.d = p.dmu; a.atap = p.atap; a.JT = p.JT; a.pitch = p.pitch;
+  auto kern = k_conv_sfft<R, NMU, JR>;
+  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem1));
+  dim3 grid((unsigned)((p.J + p.JT - 1) / p.JT));
+  kern<<<grid, 256, p.smem1, st>>>(a);
+  CK(cudaGetLastError());
+  return SOI_OK;
+}
+
+template <typename R>
+int launch_conv_r(Plan &p, const void *alpha, void *T, cudaStream_t st)
+{
+  const bool big = sizeof(R) == 8;
+  switch (p.nmu) {
+    case 2: return big ? launch_conv_t<R, 2, 8>(p, alpha, T, st) : launch_conv_t<R, 2, 8>(p, alpha, T, st);
+    case 3: return launch_conv_t<R, 3, 8>(p, alpha, T, st);
+    case 5: return launch_conv_t<R, 5, 8>(p, alpha, T, st);
+    case 8: return launch_conv_t<R, 8, 4>(p, alpha, T, st);
+    case 9: return launch_conv_t<R, 9, 4>(p, alpha, T, st);
+    default: return SOI_ERR_UNSUPPORTED;
+  }
+}
+
+int jr_for(int nmu) { return nmu >= 8 ? 4 : 8; }
+bool nmu_supported(int nmu) { return nmu == 2 || nmu == 3 || nmu == 5 || nmu == 8 || nmu == 9; }
+
+template <typename R>
+int launch_seg_t(Plan &p, void *T, void *out, cudaStream_t st)
+{
+  SegArgs a;
+  a.T = T; a.out = out;
+  a.tw1 = p.d_tw1; a.perm1 = p.d_perm1; a.plan1 = p.plan1;
+  a.tw2 = p.d_tw2; a.perm2 = p.d_perm2; a.plan2 = p.plan2;
+  a.xtw_lo = p.d_xlo; a.xtw_hi = p.d_xhi; a.winv = p.d_winv; a.wsmall = p.d_wsmall;
+  a.Mh = (long long)p.Mh; a.M = (long long)p.M;
+  a.M1 = p.M1; a.M2 = p.M2; a.C1 = p.C1; a.C2 = p.C2; a.lo_bits = p.lo_bits;
+  CK(cudaFuncSetAttribute(k_seg_cols<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_c));
+  CK(cudaFuncSetAttribute(k_seg_rows_demod<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_r));
+  dim3 g1((unsigned)(p.M2 / p.C1), (unsigned)p.S);
+  k_seg_cols<R><<<g1, 256, p.smem_c, st>>>(a);
+  CK(cudaGetLastError());
+  dim3 g2((unsigned)(p.M1 / p.C2), (unsigned)p.S);
+  k_seg_rows_demod<R><<<g2, 256, p.smem_r, st>>>(a);
+  CK(cudaGetLastError());
+  return SOI_OK;
+}
+
+int run_stage1(Plan &p, const void *alpha, void *T, cudaStream_t st)
+{
+  return p.prec == SOI_PRECISION_FP64 ? launch_conv_r<double>(p, alpha, T, st)
+                                      : launch_conv_r<float>(p, alpha, T, st);
+}
+
+int run_stage2(Plan &p, void *T, void *out, cudaStream_t st)
+{
+  return p.prec == SOI_PRECISION_FP64 ? launch_seg_t<double>(p, T, out, st)
+                                      : launch_seg_t<float>(p, T, out, st);
+}
+
+int run_vlc(Plan &p, void *T, cudaStream_t st);
+
+// ---- plan construction -------------------------------------------------------
+
+int validate(const soi_desc_t *d, size_t k)
+{
+  if (!d) return SOI_ERR_INVALID;
+  if (d->P != 1 || d->rank != 0) return SOI_ERR_UNSUPPORTED;
+  if (k < 1 || d->N == 0 || d->n_mu < 1 || d->d_mu < 1 || d->B < (size_t)d->d_mu) return SOI_ERR_INVALID;
+  if (d->precision != SOI_PRECISION_FP64 && d->precision != SOI_PRECISION_SPLIT_FP32) return SOI_ERR_INVALID;
+  size_t S = k;
+  if (d->N % S) return SOI_ERR_INVALID;
+  size_t M = d->N / S;
+  if (M % (size_t)d->d_mu) return SOI_ERR_INVALID;              // M' = n*M/d integral
+  if (M < d->B) return SOI_ERR_INVALID;                         // .cpp:89-94
+  if (!nmu_supported(d->n_mu)) return SOI_ERR_UNSUPPORTED;
+  if (S > 256 || S < 2) return SOI_ERR_UNSUPPORTED;
+  return SOI_OK;
+}
+
+int choose_split(Plan &p)
+{
+  // M' = M1*M2; pass-1 tile M1 x C1, pass-2 tile M2 x C2; each <= ~110 KB and
+  // C*elem >= 32 bytes (a full DRAM sector per row of the tile).
+  const size_t budget = p.elem == 16 ? 200 * 1024 : 110 * 1024;
+  const int cmin = (int)(32 / p.elem);
+  long long best = -1;
+  double bestscore = 1e300;
+  const long long Mh = (long long)p.Mh;
+  for (long long m1 = 2; m1 * 2 <= Mh; ++m1) {
+    if (Mh % m1) continue;
+    long long m2 = Mh / m1;
+    if (m1 > 16384 || m2 > 16384) continue;
+    FftPlan a, b;
+    if (!make_fft_plan((int)m1, a) || !make_fft_plan((int)m2, b)) continue;
+    if ((size_t)m1 * (cmin + 1) * p.elem > budget || (size_t)m2 * (cmin + 1) * p.elem > budget) continue;
+    if (m2 % cmin || m1 % cmin) continue;
+    double score = fabs(log((double)m1 / (double)m2) - 0.2);
+    if (score < bestscore) { bestscore = score; best = m1; }
+  }
+  if (best < 0) return SOI_ERR_UNSUPPORTED;
+  p.M1 = (int)best;
+  p.M2 = (int)(Mh / best);
+  p.C1 = cmin;
+  p.C2 = cmin;
+  // grow the column count while the tile stays in budget (fewer, fuller CTAs)
+  while ((size_t)p.M1 * (2 * p.C1 + 1) * p.elem <= budget && p.M2 % (2 * p.C1) == 0 && p.C1 < 16) p.C1 *= 2;
+  while ((size_t)p.M2 * (2 * p.C2 + 1) * p.elem <= budget && p.M1 % (2 * p.C2) == 0 && p.C2 < 16) p.C2 *= 2;
+  make_fft_plan(p.M1, p.plan1);
+  make_fft_plan(p.M2, p.plan2);
+  p.smem_c = (size_t)p.M1 * (p.C1 + 1) * p.elem;
+  p.smem_r = (size_t)p.M2 * (p.C2 + 1) * p.elem;
+  return SOI_OK;
+}
+
+template <typename R>
+int build_tables(Plan &p)
+{
+  std::vector<long double> filt, phr, phi, wir, wii;
+  host_tables(p.N, p.S, p.nmu, p.dmu, p.B, p.tau, p.sigma, p.atap, &filt, &phr, &phi, &wir, &wii);
+  std::vector<R> f(filt.size());
+  for (size_t i = 0; i < filt.size(); ++i) f[i] = (R)filt[i];
+  std::vector<R> ph, wi;
+  round_complex<R>(phr, phi, ph);
+  round_complex<R>(wir, wii, wi);
+  int rc;
+  if ((rc = upload(&p.d_filt, f.data(), f.size() * sizeof(R)))) return rc;
+  if ((rc = upload(&p.d_phase, ph.data(), ph.size() * sizeof(R)))) return rc;
+  if ((rc = upload(&p.d_winv, wi.data(), wi.size() * sizeof(R)))) return rc;
+  std::vector<R> tS = roots_table<R>((long long)p.S), t1 = roots_table<R>(p.M1), t2 = roots_table<R>(p.M2);
+  std::vector<R> w7 = roots_table<R>(7);
+  if ((rc = upload(&p.d_twS, tS.data(), tS.size() * sizeof(R)))) return rc;
+  if ((rc = upload(&p.d_tw1, t1.data(), t1.size() * sizeof(R)))) return rc;
+  if ((rc = upload(&p.d_tw2, t2.data(), t2.size() * sizeof(R)))) return rc;
+  if ((rc = upload(&p.d_wsmall, w7.data(), w7.size() * sizeof(R)))) return rc;
+  std::vector<int> pS = digit_reversal(p.planS), p1 = digit_reversal(p.plan1), p2 = digit_reversal(p.plan2);
+  if ((rc = upload((void **)&p.d_permS, pS.data(), pS.size() * sizeof(int)))) return rc;
+  if ((rc = upload((void **)&p.d_perm1, p1.data(), p1.size() * sizeof(int)))) return rc;
+  if ((rc = upload((void **)&p.d_perm2, p2.data(), p2.size() * sizeof(int)))) return rc;
+  // cross twiddles w_{M'}^e = hi[e >> lo_bits] * lo[e & mask], FP64
+  const long long Mh = (long long)p.Mh;
+  const long long nlo = 1LL << p.lo_bits, nhi = (Mh + nlo - 1) / nlo + 1;
+  std::vector<double> lo(2 * nlo), hi(2 * nhi);
+  for (long long e = 0; e < nlo; ++e) {
+    long double a = -2.0L * kPi * (long double)(e % Mh) / (long double)Mh;
+    lo[2 * e] = (double)cosl(a); lo[2 * e + 1] = (double)sinl(a);
+  }
+  for (long long h = 0; h < nhi; ++h) {
+    long double a = -2.0L * kPi * (long double)((h * nlo) % Mh) / (long double)Mh;
+    hi[2 * h] = (double)cosl(a); hi[2 * h + 1] = (double)sinl(a);
+  }
+  if ((rc = upload((void **)&p.d_xlo, lo.data(), lo.size() * sizeof(double)))) return rc;
+  if ((rc = upload((void **)&p.d_xhi, hi.data(), hi.size() * sizeof(double)))) return rc;
+  return SOI_OK;
+}
+
+void free_plan(Plan *p)
+{
+  if (!p) return;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(p->device);
+  void *bufs[] = { p->d_filt, p->d_phase, p->d_twS, p->d_tw1, p->d_tw2, p->d_winv, p->d_wsmall,
+                   p->d_permS, p->d_perm1, p->d_perm2, p->d_xlo, p->d_xhi, p->d_T, p->d_io,
+                   p->d_vlc_x, p->d_vlc_words, p->d_vlc_n, p->d_vlc_emax };
+  for (void *b : bufs) if (b) cudaFree(b);
+  for (auto &e : p->ev) if (e) cudaEventDestroy(e);
+  if (p->own_stream && p->stream) cudaStreamDestroy(p->stream);
+  cudaSetDevice(cur);
+  delete p;
+}
+
+// Geometry of the plan (no CUDA calls): tile shapes, FFT factorisations.
+int plan_geometry(const soi_desc_t *d, size_t k, Plan &p)
+{
+  int rc = validate(d, k);
+  if (rc) return rc;
+  p.device = d->device;
+  p.prec = d->precision;
+  p.elem = p.prec == SOI_PRECISION_FP64 ? 16 : 8;
+  p.N = d->N; p.S = k; p.M = d->N / k; p.nmu = d->n_mu; p.dmu = d->d_mu;
+  p.Mh = (size_t)p.nmu * p.M / (size_t)p.dmu; p.J = p.M / (size_t)p.dmu;
+  p.B = d->B; p.tau = d->tau; p.sigma = d->sigma;
+  p.atap = (int)((d->B + d->d_mu - 1) / d->d_mu);
+  p.JR = jr_for(p.nmu);
+  p.pitch = (int)p.S + 1;
+  if (!make_fft_plan((int)p.S, p.planS)) return SOI_ERR_UNSUPPORTED;
+  // stage-1 tile: JT output groups x all S columns, bounded by the thread
+  // count (256 / S groups of JR), shared memory and the circular wrap
+  long long jt = (long long)(256 / (int)p.S) * p.JR;
+  const size_t budget1 = 200 * 1024 - p.S * (p.elem + sizeof(int));
+  long long jt_smem = (long long)(budget1 / ((size_t)p.nmu * p.pitch * p.elem)) / p.JR * p.JR;
+  long long jt_wrap = ((long long)p.J - p.atap - p.JR) / p.JR * p.JR;
+  jt = std::min(jt, std::min(jt_smem, jt_wrap));
+  if (jt < p.JR) return SOI_ERR_UNSUPPORTED;
+  p.JT = (int)jt;
+  p.smem1 = (size_t)p.nmu * p.JT * p.pitch * p.elem + p.S * (p.elem + sizeof(int));
+  return choose_split(p);
+}
+
+int init_plan(soi_desc_t *d, size_t k)
+{
+  Plan *p = new Plan();
+  int rc = plan_geometry(d, k, *p);
+  if (rc) { delete p; return rc; }
+  cudaError_t ce = cudaSetDevice(d->device);
+  if (ce != cudaSuccess) { delete p; return SOI_ERR_CUDA; }
+  rc = p->prec == SOI_PRECISION_FP64 ? build_tables<double>(*p) : build_tables<float>(*p);
+  if (rc) { free_plan(p); return rc; }
+  if (cudaMalloc(&p->d_T, p->S * p->Mh * p->elem) != cudaSuccess) { free_plan(p); return SOI_ERR_CUDA; }
+  if (d->stream) {
+    p->stream = (cudaStream_t)d->stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess) { free_plan(p); return SOI_ERR_CUDA; }
+    p->own_stream = true;
+  }
+  for (auto &e : p->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) { free_plan(p); return SOI_ERR_CUDA; }
+  d->plan = p;
+  return SOI_OK;
+}
+
+Plan *plan_of(soi_desc_t *d) { return d ? (Plan *)d->plan : nullptr; }
+
+int compute_impl(soi_desc_t *d, void *alpha, bool stage1_only)
+{
+  Plan *p = plan_of(d);
+  if (!p) return SOI_ERR_NOT_INITIALISED;
+  if (cudaSetDevice(p->device) != cudaSuccess) return SOI_ERR_CUDA;
+  cudaStream_t st = p->stream;
+  const size_t bytes = p->N * p->elem;
+  void *io = alpha;
+  if (!d->device_ptr) {
+    if (!p->d_io) CK(cudaMalloc(&p->d_io, bytes));
+    io = p->d_io;
+    CK(cudaMemcpyAsync(io, alpha, bytes, cudaMemcpyHostToDevice, st));
+  }
+  int rc;
+  if (p->timing) CK(cudaEventRecord(p->ev[0], st));
+  if ((rc = run_stage1(*p, io, p->d_T, st))) return rc;
+  if (p->timing) CK(cudaEventRecord(p->ev[1], st));
+  if (stage1_only) {
+    CK(cudaStreamSynchronize(st));
+    return SOI_OK;
+  }
+  if (d->use_vlc && (rc = run_vlc(*p, p->d_T, st))) return rc;
+  if (p->timing) CK(cudaEventRecord(p->ev[2], st));
+  if ((rc = run_stage2(*p, p->d_T, io, st))) return rc;
+  if (p->timing) CK(cudaEventRecord(p->ev[3], st));
+  if (!d->device_ptr) CK(cudaMemcpyAsync(alpha, io, bytes, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (p->timing) {
+    cudaEventElapsedTime(&p->ms[0], p->ev[0], p->ev[1]);
+    cudaEventElapsedTime(&p->ms[2], p->ev[1], p->ev[2]);
+    cudaEventElapsedTime(&p->ms[1], p->ev[2], p->ev[3]);
+    cudaEventElapsedTime(&p->ms[3], p->ev[0], p->ev[3]);
+  }
+  return SOI_OK;
+}
+
+// ---- VLC on the transposed data (pfft.c:316-353, 390-447, 476-543, 618-632) --
+// With one process the all-to-all is the identity, so the round trip is
+// max_exponent per segment -> global max -> compress -> decompress, one chunk
+// per segment (chunk length l = M'/P = M').
+int run_vlc(Plan &p, void *T, cudaStream_t st)
+{
+  const int len = (int)(2 * p.Mh);
+  if (len % 16) return SOI_ERR_UNSUPPORTED;
+  const int ns = (int)p.S;
+  if (!p.d_vlc_words) {
+    p.vlc_stride = (long)(4 * p.Mh + 64);
+    CK(cudaMalloc(&p.d_vlc_words, (size_t)p.vlc_stride * ns * sizeof(int)));
+    CK(cudaMalloc(&p.d_vlc_n, ns * sizeof(int)));
+    CK(cudaMalloc(&p.d_vlc_emax, (ns + 1) * sizeof(int)));
+    if (p.prec != SOI_PRECISION_FP64) CK(cudaMalloc(&p.d_vlc_x, (size_t)len * ns * sizeof(double)));
+  }
+  double *x = p.prec == SOI_PRECISION_FP64 ? (double *)T : p.d_vlc_x;
+  if (p.prec != SOI_PRECISION_FP64) {
+    vlc_promote<<<1024, 256, 0, st>>>((const float *)T, x, (long long)len * ns);
+    CK(cudaGetLastError());
+  }
+  vlc_max_exponent_kernel<<<ns, 256, 0, st>>>(x, len, p.d_vlc_emax);
+  CK(cudaGetLastError());
+  vlc_global_max<<<1, 256, 0, st>>>(p.d_vlc_emax, ns, p.d_vlc_emax + ns);
+  CK(cudaGetLastError());
+  dim3 gv(64, (unsigned)ns);
+  vlc_compress_kernel<<<gv, 256, vlc_compress_smem(), st>>>(x, len, 0, p.d_vlc_emax + ns, p.d_vlc_emax,
+                                                           p.d_vlc_words, p.vlc_stride, p.d_vlc_n);
+  CK(cudaGetLastError());
+  vlc_decompress_kernel<<<gv, 256, vlc_decompress_smem(), st>>>(p.d_vlc_words, p.vlc_stride, len, nullptr,
+                                                               p.d_vlc_emax + ns, p.d_vlc_emax, x);
+  CK(cudaGetLastError());
+  if (p.prec != SOI_PRECISION_FP64) {
+    vlc_demote<<<1024, 256, 0, st>>>(x, (float *)T, (long long)len * ns);
+    CK(cudaGetLastError());
+  }
+  return SOI_OK;
+}
+
+void die_on(int rc, const char *what)
+{
+  if (rc == SOI_OK) return;
+  fprintf(stderr, "%s: %s\n", what, soi_status_string(rc));
+  exit(-1);
+}
+
+}  // namespace
+
+// ============================================================ C ABI ==========
+
+extern "C" {
+
+const char *soi_b200_version(void) { return "soi_b200 0.1 (sm_100a)"; }
+
+const char *soi_status_string(int s)
+{
+  switch (s) {
+    case SOI_OK: return "ok";
+    case SOI_ERR_INVALID: return "invalid parameters";
+    case SOI_ERR_UNSUPPORTED: return "configuration not supported by this build";
+    case SOI_ERR_CUDA: return "CUDA runtime error";
+    case SOI_ERR_NOT_INITIALISED: return "descriptor not initialised";
+    case SOI_ERR_TIMEOUT: return "device-side wait timed out";
+    default: return "unknown status";
+  }
+}
+
+void set_default_soi_descriptor(soi_desc_t *d)
+{
+  memset(d, 0, sizeof(*d));
+  d->n_mu = 5;                 // pfft.c:87-91
+  d->d_mu = 4;
+  d->tau = 928 / 1024.;
+  d->sigma = 373.7314;
+  d->B = 72;
+  d->use_vlc = 0;              // pfft.c:93-94
+  d->comm_to_comp_cost_ratio = 1;
+  d->P = 1;
+  d->rank = 0;
+  d->precision = SOI_PRECISION_FP64;
+}
+
+int soi_init_status(soi_desc_t *d, soi_comm_t comm, cfft_size_t k)
+{
+  if (!d) return SOI_ERR_INVALID;
+  d->comm = comm;
+  d->k = k;
+  if (d->plan) { free_plan((Plan *)d->plan); d->plan = nullptr; }
+  int rc = init_plan(d, k);
+  if (rc == SOI_OK) {
+    free(d->segmentBoundaries);
+    d->segmentBoundaries = (int *)malloc(sizeof(int) * 2);   // pfft.c:144-147 with P = 1
+    d->segmentBoundaries[0] = 0;
+    d->segmentBoundaries[1] = (int)k;
+  }
+  d->last_status = rc;
+  return rc;
+}
+
+void init_soi_descriptor(soi_desc_t *d, soi_comm_t comm, cfft_size_t k)
+{
+  die_on(soi_init_status(d, comm, k), "init_soi_descriptor");
+}
+
+int soi_compute_status(soi_desc_t *d, void *alpha)
+{
+  if (!d) return SOI_ERR_INVALID;
+  int rc = alpha ? compute_impl(d, alpha, false) : SOI_ERR_INVALID;
+  d->last_status = rc;
+  return rc;
+}
+
+void compute_soi(soi_desc_t *d, void *alpha) { die_on(soi_compute_status(d, alpha), "compute_soi"); }
+
+int soi_filter_subsampling_status(soi_desc_t *d, void *alpha)
+{
+  if (!d) return SOI_ERR_INVALID;
+  int rc = alpha ? compute_impl(d, alpha, true) : SOI_ERR_INVALID;
+  d->last_status = rc;
+  return rc;
+}
+
+void parallel_filter_subsampling(soi_desc_t *d, void *alpha)
+{
+  die_on(soi_filter_subsampling_status(d, alpha), "parallel_filter_subsampling");
+}
+
+int soi_get_transposed(soi_desc_t *d, void *dst)
+{
+  Plan *p = plan_of(d);
+  if (!p) return SOI_ERR_NOT_INITIALISED;
+  if (cudaSetDevice(p->device) != cudaSuccess) return SOI_ERR_CUDA;
+  CK(cudaMemcpyAsync(dst, p->d_T, p->S * p->Mh * p->elem,
+                     d->device_ptr ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  return SOI_OK;
+}
+
+int soi_free_status(soi_desc_t *d)
+{
+  if (!d) return SOI_ERR_INVALID;
+  if (d->plan) free_plan((Plan *)d->plan);
+  d->plan = nullptr;
+  free(d->segmentBoundaries);
+  d->segmentBoundaries = nullptr;
+  return SOI_OK;
+}
+
+void free_soi_descriptor(soi_desc_t *d) { soi_free_status(d); }
+
+int soi_filter_subsample_device(soi_desc_t *d, const void *alpha_dev, void *T_dev)
+{
+  Plan *p = plan_of(d);
+  if (!p) return SOI_ERR_NOT_INITIALISED;
+  if (cudaSetDevice(p->device) != cudaSuccess) return SOI_ERR_CUDA;
+  return run_stage1(*p, alpha_dev, T_dev, p->stream);
+}
+
+int soi_segment_fft_demod_device(soi_desc_t *d, void *T_dev, void *out_dev)
+{
+  Plan *p = plan_of(d);
+  if (!p) return SOI_ERR_NOT_INITIALISED;
+  if (cudaSetDevice(p->device) != cudaSuccess) return SOI_ERR_CUDA;
+  return run_stage2(*p, T_dev, out_dev, p->stream);
+}
+
+int soi_plan_geometry(const soi_desc_t *d, cfft_size_t k, long long *info)
+{
+  if (!info) return SOI_ERR_INVALID;
+  Plan p;
+  int rc = plan_geometry(d, k, p);
+  if (rc) return rc;
+  long long v[16] = { (long long)p.S, (long long)p.M, (long long)p.Mh, p.JT, p.atap, p.JR,
+                      (long long)p.smem1, p.M1, p.M2, p.C1, p.C2, (long long)p.smem_c,
+                      (long long)p.smem_r, p.planS.nst, p.plan1.nst, p.plan2.nst };
+  memcpy(info, v, sizeof(v));
+  return SOI_OK;
+}
+
+int soi_set_timing(soi_desc_t *d, int enable)
+{
+  Plan *p = plan_of(d);
+  if (!p) return SOI_ERR_NOT_INITIALISED;
+  p->timing = enable != 0;
+  return SOI_OK;
+}
+
+int soi_last_timings(soi_desc_t *d, float *ms4)
+{
+  Plan *p = plan_of(d);
+  if (!p) return SOI_ERR_NOT_INITIALISED;
+  for (int i = 0; i < 4; ++i) ms4[i] = p->ms[i];
+  return SOI_OK;
+}
+
+int soi_window_tables(cfft_size_t N, cfft_size_t S, int n_mu, int d_mu, cfft_size_t B, double tau,
+                      double sigma, double *filt, double *phase, double *W_inv)
+{
+  if (!N || !S || N % S || n_mu < 1 || d_mu < 1 || B < (size_t)d_mu) return SOI_ERR_INVALID;
+  std::vector<long double> f, pr, pi, wr, wi;
+  host_tables(N, S, n_mu, d_mu, B, tau, sigma, 0, filt ? &f : nullptr, phase ? &pr : nullptr,
+              phase ? &pi : nullptr, W_inv ? &wr : nullptr, W_inv ? &wi : nullptr);
+  if (filt) for (size_t i = 0; i < f.size(); ++i) filt[i] = (double)f[i];
+  if (phase) for (size_t i = 0; i < pr.size(); ++i) { phase[2 * i] = (double)pr[i]; phase[2 * i + 1] = (double)pi[i]; }
+  if (W_inv) for (size_t i = 0; i < wr.size(); ++i) { W_inv[2 * i] = (double)wr[i]; W_inv[2 * i + 1] = (double)wi[i]; }
+  return SOI_OK;
+}
+
+int soi_vlc_words(int len, int e_max, int e_max_i)
+{
+  const int delta = e_max - e_max_i;
+  const int i1 = (52 + 3 - 31) - delta, i2 = std::min(32, 52 + 3 - delta);
+  if (i2 <= 0) return 0;
+  const int nb = (i1 > 0 ? i1 : 0) + i2;
+  const long long lanes = (long long)(len / 16) * nb;
+  long long w = (lanes + 31) / 32 * 16;
+  w += ((long long)(len % 16) * nb + 31) / 32;
+  return (int)w;
+}
+
+int soi_vlc_max_exponent_device(const double *x, int len, int nchunks, int *e_max_out, void *stream)
+{
+  if (!x || !e_max_out || len <= 0 || nchunks <= 0) return SOI_ERR_INVALID;
+  vlc_max_exponent_kernel<<<nchunks, 256, 0, (cudaStream_t)stream>>>(x, len, e_max_out);
+  CK(cudaGetLastError());
+  return SOI_OK;
+}
+
+int soi_vlc_compress_device(const double *x, int len, int nchunks, int e_max, const int *e_max_i,
+                            int *words, long stride_words, int *nwords, void *stream)
+{
+  if (!x || !e_max_i || !words || !nwords || len <= 0 || nchunks <= 0) return SOI_ERR_INVALID;
+  if (len % 16) return SOI_ERR_UNSUPPORTED;
+  dim3 g(64, (unsigned)nchunks);
+  vlc_compress_kernel<<<g, 256, 0, (cudaStream_t)stream>>>(x, len, e_max, nullptr, e_max_i, words, stride_words, nwords);
+  CK(cudaGetLastError());
+  return SOI_OK;
+}
+
+int soi_vlc_decompress_device(const int *words, long stride_words, int len, int nchunks, int e_max,
+                              const int *e_max_i, double *out, void *stream)
+{
+  if (!words || !e_max_i || !out || len <= 0 || nchunks <= 0) return SOI_ERR_INVALID;
+  if (len % 16) return SOI_ERR_UNSUPPORTED;
+  int *d_emax = nullptr;
+  CK(cudaMallocAsync(&d_emax, sizeof(int), (cudaStream_t)stream));
+  CK(cudaMemcpyAsync(d_emax, &e_max, sizeof(int), cudaMemcpyHostToDevice, (cudaStream_t)stream));
+  dim3 g(64, (unsigned)nchunks);
+  vlc_decompress_kernel<<<g, 256, 0, (cudaStream_t)stream>>>(words, stride_words, len, nullptr, d_emax, e_max_i, out);
+  CK(cudaGetLastError());
+  CK(cudaFreeAsync(d_emax, (cudaStream_t)stream));
+  CK(cudaStreamSynchronize((cudaStream_t)stream));
+  return SOI_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,207 @@
+// vlc_kernels.cuh -- the variable-length compression of compress.c on the GPU,
+// bit-exact to the reference's stream for chunks whose length (in doubles) is
+// a multiple of 16, which is every chunk on the SOI path (2*M'/P doubles).
+//
+// Stream format (compress.c:170-203,227-328): element e = 16*g + L goes to
+// lane L; each element contributes one field of nb = max(i1Len,0) + i2Len
+// bits, i1 (i1Len bits) then i2 (i2Len bits), appended MSB-first to the
+// lane's 32-bit words; lane L's word w is stored at out[16*w + L]; a partial
+// last word group is flushed with zero padding.  Because every lane receives
+// the same number of bits, bit b of lane L's stream is simply bit (b mod 32,
+// from the top) of word floor(b/32) -- so each output word can be assembled
+// independently from the (at most ceil(32/nb)+1) fields it overlaps, and each
+// element decoded independently from the (at most 3) words its field spans.
+// That is what these kernels do: one thread per word, one thread per element.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <limits.h>
+#include <stdint.h>
+
+namespace soi {
+
+constexpr int kVlcLanes = 16;
+
+struct VlcBits {
+  int i1Len, i2Len, nb;
+  double e1, e2, e3;        // quantisation scales (compress.c:214-216)
+  double d1, d2;            // reconstruction scales (compress.c:430-431)
+};
+
+__device__ __forceinline__ VlcBits vlc_bits(int e_max, int e_max_i)
+{
+  VlcBits b;
+  const int delta = e_max - e_max_i;
+  b.i1Len = (52 + 3 - 31) - delta;                          // compress.c:207
+  b.i2Len = min(32, 52 + 3 - delta);                        // compress.c:208
+  b.nb = (b.i1Len > 0 ? b.i1Len : 0) + b.i2Len;
+  b.e1 = ldexp(1.0, (52 - 31) - e_max);
+  b.e2 = ldexp(1.0, 52 - e_max);
+  b.e3 = ldexp(1.0, 31);
+  b.d1 = ldexp(1.0, e_max - (52 - 31));
+  b.d2 = ldexp(1.0, e_max - 52);
+  return b;
+}
+
+// The packed field of one element (vector-path rounding: round-to-nearest-even
+// for i1, a fused multiply-subtract then round-to-nearest-even for i2,
+// compress.c:235-280).
+__device__ __forceinline__ uint64_t vlc_field(double x, const VlcBits &b)
+{
+  const double r1 = rint(__dmul_rn(x, b.e1));
+  const double r2 = fma(x, b.e2, -__dmul_rn(r1, b.e3));
+  const int32_t i1 = (int32_t)r1;
+  const int32_t i2 = (int32_t)rint(r2);
+  const uint64_t m2 = b.i2Len >= 32 ? 0xFFFFFFFFull : ((1ull << b.i2Len) - 1);
+  uint64_t f = (uint64_t)(uint32_t)i2 & m2;
+  if (b.i1Len > 0) {
+    const uint64_t m1 = (1ull << b.i1Len) - 1;
+    f |= ((uint64_t)(uint32_t)i1 & m1) << b.i2Len;
+  }
+  return f;
+}
+
+__global__ void vlc_promote(const float *in, double *out, long long n)
+{
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = (double)in[i];
+}
+
+__global__ void vlc_demote(const double *in, float *out, long long n)
+{
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = (float)in[i];
+}
+
+// compress.c:11-131: per chunk (blockIdx.x), max biased exponent - 1023.
+__global__ void vlc_max_exponent_kernel(const double *x, int len, int *e_max)
+{
+  const double *c = x + (size_t)blockIdx.x * len;
+  int m = 0;
+  for (int i = threadIdx.x; i < len; i += blockDim.x) {
+    const unsigned long long u = (unsigned long long)__double_as_longlong(c[i]);
+    m = max(m, (int)((u >> 52) & 0x7FF));
+  }
+  for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  __shared__ int wm[32];
+  if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    int v = threadIdx.x < (blockDim.x + 31) / 32 ? wm[threadIdx.x] : 0;
+    for (int o = 16; o; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (threadIdx.x == 0) e_max[blockIdx.x] = v - 1023;
+  }
+}
+
+// max over chunks (pfft.c:340-343, after the MPI_Allreduce MAX of :331-333)
+__global__ void vlc_global_max(const int *e, int n, int *out)
+{
+  int m = INT_MIN;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) m = max(m, e[i]);
+  for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  __shared__ int wm[32];
+  if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    int v = threadIdx.x < (blockDim.x + 31) / 32 ? wm[threadIdx.x] : INT_MIN;
+    for (int o = 16; o; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (threadIdx.x == 0) *out = v;
+  }
+}
+
+inline size_t vlc_compress_smem() { return 0; }
+inline size_t vlc_decompress_smem() { return 0; }
+
+// Words per lane for a chunk of len doubles (len % 16 == 0).
+__host__ __device__ __forceinline__ long long vlc_words_per_lane(int len, int nb)
+{
+  const long long groups = len / kVlcLanes;
+  return (groups * nb + 31) / 32;
+}
+
+// compress.c:205-372, one chunk per blockIdx.y (grid-stride over words in x).
+// e_max = *e_max_dev when given, else e_max_host; e_max_i[c] per chunk.
+__global__ void vlc_compress_kernel(const double *x, int len, int e_max_host, const int *e_max_dev,
+                                    const int *e_max_i, int *words, long stride, int *nwords)
+{
+  const int c = blockIdx.y;
+  const int e_max = e_max_dev ? *e_max_dev : e_max_host;
+  const VlcBits b = vlc_bits(e_max, e_max_i[c]);
+  const double *xc = x + (size_t)c * len;
+  int *wc = words + (size_t)c * stride;
+  if (b.i2Len <= 0) {                        // compress.c:210-212
+    if (blockIdx.x == 0 && threadIdx.x == 0) nwords[c] = 0;
+    return;
+  }
+  const long long nwl = vlc_words_per_lane(len, b.nb);
+  const long long total = nwl * kVlcLanes;
+  const long long groups = len / kVlcLanes;
+  if (blockIdx.x == 0 && threadIdx.x == 0) nwords[c] = (int)total;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const long long w = idx / kVlcLanes;
+    const int L = (int)(idx % kVlcLanes);
+    const long long sb = 32 * w;                // first stream bit of the word
+    long long g = sb / b.nb;
+    int skip = (int)(sb - g * b.nb);           // bits of field g already used
+    uint32_t word = 0;
+    int have = 0;                               // bits placed so far (from the top)
+    while (have < 32 && g < groups) {
+      const uint64_t f = vlc_field(xc[g * kVlcLanes + L], b);
+      const int avail = b.nb - skip;            // remaining bits of this field
+      const int take = min(avail, 32 - have);
+      // bits [avail-1 .. avail-take] of the field's remaining low bits
+      const uint64_t part = (f >> (avail - take)) & ((1ull << take) - 1);
+      word |= (uint32_t)(part << (32 - have - take));
+      have += take;
+      ++g;
+      skip = 0;
+    }
+    wc[idx] = (int)word;
+  }
+}
+
+// compress.c:428-544 (vector body, :395-426 and :450-489), one element per
+// thread, one chunk per blockIdx.y.
+__global__ void vlc_decompress_kernel(const int *words, long stride, int len, const int *unused,
+                                      const int *e_max_dev, const int *e_max_i, double *out)
+{
+  (void)unused;
+  const int c = blockIdx.y;
+  const int e_max = *e_max_dev;
+  const VlcBits b = vlc_bits(e_max, e_max_i[c]);
+  double *oc = out + (size_t)c * len;
+  const uint32_t *wc = reinterpret_cast<const uint32_t *>(words + (size_t)c * stride);
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < len;
+       e += (long long)gridDim.x * blockDim.x) {
+    if (b.i2Len <= 0) { oc[e] = 0.0; continue; }
+    const long long g = e / kVlcLanes;
+    const int L = (int)(e % kVlcLanes);
+    const long long sb = g * b.nb;
+    long long w = sb / 32;
+    int off = (int)(sb - 32 * w);               // bit offset from the top of word w
+    // gather nb bits MSB-first into f
+    uint64_t f = 0;
+    int need = b.nb;
+    while (need > 0) {
+      const uint32_t word = __ldg(wc + w * kVlcLanes + L);
+      const int avail = 32 - off;
+      const int take = min(avail, need);
+      const uint32_t part = (uint32_t)(((uint64_t)word >> (avail - take)) & ((1ull << take) - 1));
+      f = (f << take) | part;
+      need -= take;
+      ++w;
+      off = 0;
+    }
+    int32_t i1 = 0;
+    if (b.i1Len > 0) {
+      const uint32_t top = (uint32_t)(f >> b.i2Len);
+      i1 = (int32_t)(top << (32 - b.i1Len)) >> (32 - b.i1Len);
+    }
+    const uint32_t low = (uint32_t)(f & (b.i2Len >= 32 ? 0xFFFFFFFFull : ((1ull << b.i2Len) - 1)));
+    const int32_t i2 = b.i2Len >= 32 ? (int32_t)low : ((int32_t)(low << (32 - b.i2Len)) >> (32 - b.i2Len));
+    oc[e] = fma((double)i1, b.d1, __dmul_rn((double)i2, b.d2));
+  }
+}
+
+}  // namespace soi

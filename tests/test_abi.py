@@ -1,0 +1,104 @@
+"""CPU tests of the C ABI boundary: the library loads, exports every function
+include/soi_b200.h declares, validates arguments before touching a GPU, and
+its host-side tables equal the reference's window (pfft.c:42-82)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import soi_fft_b200 as sb
+from oracle import oracle
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    src = open(os.path.join(ROOT, "include", "soi_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = re.findall(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_]*\s*\*?\s*([A-Za-z_][A-Za-z0-9_]*)\s*\(",
+                       src, flags=re.M)
+    return sorted(set(n for n in names if n not in ("if", "defined")))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = sb.lib()
+    names = declared_functions()
+    assert "compute_soi" in names and "init_soi_descriptor" in names
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_reference_entry_points_present():
+    # soi.h:272-280
+    for n in ("set_default_soi_descriptor", "init_soi_descriptor", "compute_soi",
+              "free_soi_descriptor", "parallel_filter_subsampling"):
+        assert hasattr(sb.lib(), n)
+
+
+def test_defaults_match_reference():
+    d = sb.SoiDescriptor()
+    # pfft.c:87-94
+    assert (d.n_mu, d.d_mu, d.B) == (5, 4, 72)
+    assert d.tau == 928 / 1024.
+    assert d.sigma == 373.7314
+    assert d.use_vlc == 0 and d.comm_to_comp_cost_ratio == 1
+    assert d.P == 1 and d.rank == 0
+
+
+@pytest.mark.parametrize("fields,k,status", [
+    (dict(N=1 << 16, P=2), 8, 2),            # multi-rank: not built here
+    (dict(N=1 << 16), 0, 1),                 # k = 0
+    (dict(N=1000), 8, 1),                    # S does not divide N
+    (dict(N=1 << 16, n_mu=7, d_mu=4), 8, 2),  # oversampling pair not built
+    (dict(N=1 << 8), 8, 1),                  # M < B (.cpp:89-94)
+    (dict(N=1 << 16, precision=5), 8, 1),
+])
+def test_init_rejects_before_touching_the_gpu(fields, k, status):
+    d = sb.SoiDescriptor(**fields)
+    with pytest.raises(sb.SoiError) as e:
+        d.init(k)
+    assert e.value.status == status
+
+
+def test_void_entry_point_exits_like_the_reference(tmp_path):
+    # init_soi_descriptor on an invalid descriptor prints and exits(-1), as the
+    # reference does for unsupported sizes (.cpp:543-548)
+    import subprocess
+    import sys
+    code = ("import ctypes, soi_fft_b200 as sb\n"
+            "d = sb.SoiDescriptor(N=1000)\n"
+            "sb.lib().init_soi_descriptor.argtypes=[ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]\n"
+            "sb.lib().init_soi_descriptor(ctypes.byref(d._d), None, 8)\n"
+            "print('survived')\n")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True)
+    assert r.returncode == 255 and "survived" not in r.stdout
+    assert "invalid parameters" in r.stderr
+
+
+@pytest.mark.parametrize("N,S,n,d,B,tau,sigma", [
+    (1 << 16, 8, 5, 4, 72, 928 / 1024., 373.7314),
+    (1 << 18, 64, 5, 4, 72, 928 / 1024., 373.7314),
+    (1 << 16, 16, 5, 4, 44, 512 / 1024., 121.0936),
+    (7 << 14, 8, 8, 7, 72, 928 / 1024., 373.7314),
+])
+def test_factorised_window_equals_reference_window(N, S, n, d, B, tau, sigma):
+    filt, phase, winv = sb.window_tables(N, S, n, d, B, tau, sigma)
+    w = oracle.w_table(N, S, n, d, B, tau, sigma)            # [theta][kk][s]
+    wf = np.transpose(phase[None, :, :] * filt, (1, 0, 2))
+    # the reference rounds t in double before evaluating the window; the
+    # exact-rational tables differ from it by that rounding, ~1e-14
+    assert np.abs(wf - w).max() <= 5e-14 * np.abs(w).max()
+    W = oracle.W_inv_table(N, S, n, d, B, tau, sigma)
+    # W_inv = 1/y with y a difference of two erfc values (pfft.c:75); near the
+    # segment edges y ~ 1e-4 and the reference's double erfc loses ~1e-12
+    # relative there, the long-double tables do not
+    assert np.abs(winv - W).max() <= 1e-11 * np.abs(W).max()
+    assert np.linalg.norm(winv - W) <= 1e-12 * np.linalg.norm(W)
+
+
+@pytest.mark.parametrize("ln,emax,emaxi", [(16, 3, 3), (64, 10, 2), (4096, 20, -10), (160, 5, -40),
+                                            (32, 0, -60), (17, 3, 1)])
+def test_vlc_word_count_matches_oracle(ln, emax, emaxi):
+    assert sb.lib().soi_vlc_words(ln, emax, emaxi) == oracle.vlc_words(ln, emax, emaxi)

@@ -1,0 +1,160 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle.
+
+Plain FP64: rel-L2 <= 1e-12 against the oracle (the reference's algorithm,
+bit-identical to the reference's own sources).  Split precision (complex64
+storage, FP32 arithmetic): rel-L2 <= 1e-6 against an FP64 direct FFT."""
+import numpy as np
+import pytest
+
+import soi_fft_b200 as sb
+from oracle import oracle
+from tests.conftest import rel_l2
+from tests import signals
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+FP64_TOL = 1e-12
+SPLIT_TOL = 1e-6
+
+
+def on_gpu(x):
+    return torch.from_numpy(np.ascontiguousarray(x)).cuda()
+
+
+def max_err(y, ref):
+    # compute_normalized_inf_norm, input.c:395-425
+    return float(np.sqrt(np.max(np.abs(y - ref) ** 2) / np.max(np.abs(ref) ** 2)))
+
+
+CASES = [  # N, S, n_mu, d_mu, B, tau, sigma
+    (1 << 14, 4, 5, 4, 72, None, None),
+    (1 << 16, 8, 5, 4, 72, None, None),
+    (1 << 18, 16, 5, 4, 72, None, None),
+    (1 << 18, 64, 5, 4, 72, None, None),
+    (1 << 20, 8, 5, 4, 72, None, None),      # the reference's CPU case: N=2^20, S=8
+    (1 << 20, 128, 5, 4, 72, None, None),
+    (1 << 17, 32, 5, 4, 44, 512 / 1024, 121.0936),   # Pareto point pfft.c:121
+    (1 << 17, 16, 5, 4, 60, 0.899, 352.7647081),     # pfft.c:115
+    (7 << 14, 8, 8, 7, 72, None, None),      # mu = 8/7 (.cpp:540)
+    (1 << 18, 16, 9, 8, 72, 0.7238, 476.8683),   # mu = 9/8 (not dispatched by the reference)
+    (3 << 16, 12, 5, 4, 72, None, None),     # S not a power of two
+]
+
+
+def _kw(n, d, B, tau, sigma):
+    kw = dict(n_mu=n, d_mu=d, B=B)
+    if tau is not None:
+        kw.update(tau=tau, sigma=sigma)
+    return kw
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: "N%d_S%d_mu%d-%d_B%d" % c[:5])
+def test_fp64_matches_oracle(case):
+    N, S, n, d, B, tau, sigma = case
+    x = signals.gaussian(N, N ^ S)
+    kw = _kw(n, d, B, tau, sigma)
+    ref = oracle.compute_soi(x, S, **kw)
+    y = sb.soi_fft(on_gpu(x), S, **kw).cpu().numpy()
+    assert rel_l2(y, ref) <= FP64_TOL
+    assert max_err(y, ref) <= 10 * FP64_TOL
+
+
+@pytest.mark.parametrize("case", CASES[:8], ids=lambda c: "N%d_S%d_B%d" % (c[0], c[1], c[4]))
+def test_split_fp32_vs_fp64_direct_fft(case):
+    N, S, n, d, B, tau, sigma = case
+    x = signals.gaussian_plus_tones(N, 3 * N + S)
+    X = np.fft.fft(x)
+    y = sb.soi_fft(on_gpu(x.astype(np.complex64)), S, **_kw(n, d, B, tau, sigma)).cpu().numpy()
+    assert y.dtype == np.complex64
+    # the input itself is rounded to complex64 once; the bound covers that too
+    assert rel_l2(y.astype(np.complex128), X) <= SPLIT_TOL
+
+
+@pytest.mark.parametrize("prec", [sb.PRECISION_FP64, sb.PRECISION_SPLIT_FP32])
+def test_host_pointer_equals_device_pointer(prec):
+    N, S = 1 << 18, 16
+    dt = np.complex128 if prec == sb.PRECISION_FP64 else np.complex64
+    x = signals.gaussian(N, 5, dt)
+    d = sb.SoiDescriptor(N=N, precision=prec).init(S)
+    yh = d.compute(x.copy())
+    yd = d.compute(on_gpu(x)).cpu().numpy()
+    d.free()
+    assert np.array_equal(yh, yd)
+
+
+def test_stage1_transposed_matches_oracle():
+    N, S = 1 << 18, 32
+    x = signals.gaussian(N, 17)
+    d = sb.SoiDescriptor(N=N).init(S)
+    T = d.filter_subsampling(x.copy())
+    d.free()
+    Tref = oracle.transposed(x, S)
+    assert T.shape == Tref.shape
+    assert rel_l2(T, Tref) <= 1e-13
+
+
+def test_repeated_compute_is_deterministic():
+    N, S = 1 << 18, 16
+    x = signals.gaussian(N, 8)
+    d = sb.SoiDescriptor(N=N).init(S)
+    a = d.compute(on_gpu(x)).cpu().numpy()
+    b = d.compute(on_gpu(x)).cpu().numpy()
+    d.free()
+    assert np.array_equal(a, b)
+
+
+def test_edge_inputs():
+    N, S = 1 << 16, 8
+    d = sb.SoiDescriptor(N=N).init(S)
+    z = d.compute(np.zeros(N, np.complex128))
+    assert not np.any(z)
+    # a delta at 0 transforms to all ones
+    e = np.zeros(N, np.complex128)
+    e[0] = 1
+    assert rel_l2(d.compute(e), np.ones(N, np.complex128)) <= FP64_TOL
+    # a pure on-bin tone transforms to a single spike
+    k0 = 12345
+    t = np.exp(2j * np.pi * k0 * np.arange(N) / N)
+    Y = d.compute(t)
+    ref = np.zeros(N, np.complex128)
+    ref[k0] = N
+    assert rel_l2(Y, ref) <= FP64_TOL
+    d.free()
+
+
+def test_smallest_and_largest_segment_counts():
+    for N, S in ((1 << 13, 2), (1 << 20, 256)):
+        x = signals.gaussian(N, S)
+        y = sb.soi_fft(on_gpu(x), S).cpu().numpy()
+        assert rel_l2(y, oracle.compute_soi(x, S)) <= FP64_TOL
+
+
+@pytest.mark.parametrize("N,S", [(1 << 24, 64), (1 << 26, 128)])
+def test_large_sizes_against_cufft(N, S):
+    # size-independent checks at sizes the CPU oracle is slow for: the FP64
+    # direct FFT is cuFFT's Z2Z (called as a library, as the checker only)
+    x = signals.gaussian_plus_tones(N, N + 1)
+    xd = on_gpu(x)
+    X = torch.fft.fft(xd)
+    y64 = sb.soi_fft(xd, S)
+    assert float(torch.linalg.norm(y64 - X) / torch.linalg.norm(X)) <= FP64_TOL
+    y32 = sb.soi_fft(xd.to(torch.complex64), S).to(torch.complex128)
+    assert float(torch.linalg.norm(y32 - X) / torch.linalg.norm(X)) <= SPLIT_TOL
+    # linearity of the FP64 path: T(a x + b u) = a T(x) + b T(u)
+    u = on_gpu(signals.gaussian(N, 2))
+    a, b = 0.3 - 1.1j, 2.0 + 0.5j
+    lhs = sb.soi_fft(a * xd + b * u, S)
+    rhs = a * y64 + b * sb.soi_fft(u, S)
+    assert float(torch.linalg.norm(lhs - rhs) / torch.linalg.norm(rhs)) <= FP64_TOL
+
+
+def test_timings_reported():
+    N, S = 1 << 20, 16
+    d = sb.SoiDescriptor(N=N, precision=sb.PRECISION_SPLIT_FP32).init(S)
+    d.set_timing(True)
+    d.compute(on_gpu(signals.gaussian(N, 1, np.complex64)))
+    t = d.timings()
+    d.free()
+    assert t["stage1_ms"] > 0 and t["stage2_ms"] > 0 and t["total_ms"] >= t["stage1_ms"]

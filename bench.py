@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""bench.py -- SOI FFT on B200: GFLOP/s (5 N log2 N) at N=2^29.
+
+Workload (one step = one SOI transform of one synthetic batch):
+    N = 2^29 complex64 (4 GiB), S = 128 segments, mu = 5/4, B = 72 taps,
+    split-precision form (FP32 arithmetic, complex64 storage,
+    FP64-generated tables rounded once).  Input: seeded complex Gaussian plus
+    64 pure tones at random bin + fractional offsets with amplitudes
+    log-uniform in [1e-6, 1] (synthetic stand-in; the reference names no
+    dataset).  Inputs (4 GiB) are larger than L2 (126 MB), so no L2 flush is
+    needed between steps.
+
+value   : device-resident inputs, out-of-place transform through the C ABI
+          (soi_compute_oop_status with device pointers), CUDA events on the
+          library's stream over exactly K steps.
+e2e     : the same transform through the C ABI with host (pinned) buffers,
+          the host->device copy of the input and the device->host copy of the
+          output inside every timed step.
+fp64_plain : the plain FP64 method on the same signal at the same N.
+accuracy   : rel-L2 and max error of both forms against cuFFT's FP64 Z2Z
+             transform of the same input (the FP64 direct-FFT checker).
+roofline   : the dominant kernel (stage 1, convolution + S-point FFTs +
+             transposed store) against measured HBM bandwidth.
+cpu_baseline : the reference's own compute_soi (oracle/_ref, compiled from the
+               reference sources) on the host cores, bounded sample.
+
+--impl reference times the reference's CPU implementation alone.
+Multi-GPU (torchrun): independent replicas, one per GPU (the transform does
+not shard without an all-to-all, which this build does not use); value =
+transforms of all ranks / max-over-ranks time.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(N=1 << 29, S=128, n_mu=5, d_mu=4, B=72)
+METRIC = "GFLOP/s (5N log2 N) at N=2^29, split-FP32 vs plain FP64 GPU, at rel-L2 <=1e-6"
+CPU_SAMPLE_LOG2N = 24
+
+
+def flop(N):
+    return 5.0 * N * math.log2(N)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--log2n", type=int, default=29)
+    ap.add_argument("--segments", type=int, default=128)
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- helpers --
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [v.strip() for v in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return world, rank, local, pg
+
+
+def make_signal(N, seed, device):
+    """complex128 Gaussian + 64 tones, built on the GPU in FP64."""
+    import torch
+    g = torch.Generator(device=device).manual_seed(seed)
+    x = torch.complex(torch.randn(N, generator=g, device=device, dtype=torch.float64),
+                      torch.randn(N, generator=g, device=device, dtype=torch.float64))
+    n = torch.arange(N, device=device, dtype=torch.int64)
+    gc = torch.Generator().manual_seed(seed + 1)
+    for _ in range(64):
+        k0 = int(torch.randint(0, N, (1,), generator=gc))
+        frac = float(torch.rand(1, generator=gc, dtype=torch.float64))
+        amp = 10.0 ** float(torch.empty(1, dtype=torch.float64).uniform_(-6, 0, generator=gc))
+        ph0 = float(torch.rand(1, generator=gc, dtype=torch.float64)) * 2 * math.pi
+        m = torch.remainder(n * k0, N).to(torch.float64)
+        ph = (m + frac * n.to(torch.float64)) * (2 * math.pi / N) + ph0
+        x += amp * torch.polar(torch.ones_like(ph), ph)
+        del m, ph
+    del n
+    return x
+
+
+def cpu_baseline(log2n, S, steps, threads=None, bounded=True):
+    """The reference's compute_soi compiled from its own sources (oracle/_ref),
+    1 rank x T OpenMP threads, on a bounded sample of the workload."""
+    from oracle import oracle
+    import numpy as np
+    if not oracle.ref_available():
+        return None
+    N = 1 << log2n
+    ncpu = os.cpu_count() or 8
+    ntg = min(S // 4, 8)
+    T = threads or max(ntg, ncpu // ntg * ntg)
+    r = np.random.default_rng(1)
+    x = r.standard_normal(N) + 1j * r.standard_normal(N)
+    _, best, times = oracle.run_reference(x, 1, S, threads=T, repeat=steps, return_times=True)
+    mean = statistics.mean(times)
+    return {"value": flop(N) / mean / 1e9, "best_value": flop(N) / best / 1e9, "unit": "GFLOP/s",
+            "cores": T, "kind": "reference",
+            "sample": "reference compute_soi (pfft.c + parallel_filter_subsampling.cpp built here, "
+                      "DFTI backed by the oracle FFT, not MKL) at N=2^%d, S=%d, mu=5/4, B=72, FP64, "
+                      "1 rank x %d threads, mean of %d runs" % (log2n, S, T, steps),
+            "seconds_per_transform": mean}
+
+
+# ------------------------------------------------------------- reference ---
+
+def run_reference(args):
+    world, rank, _, pg = dist_setup(args)
+    if rank != 0:
+        return
+    log2n = min(args.log2n, CPU_SAMPLE_LOG2N)
+    res = cpu_baseline(log2n, args.segments, args.steps + args.warmup)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/soi_ref_run is not built"}))
+        return
+    line = {"metric": METRIC, "value": res["value"], "unit": "GFLOP/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": res["seconds_per_transform"] * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
+            "data": "synthetic: seeded i.i.d. complex Gaussian",
+            "config": {"workload": "SOI FFT, reference CPU path, bounded sample N=2^%d of N=2^%d" % (log2n, args.log2n),
+                       "N": 1 << log2n, "S": args.segments, "mu": "5/4", "B": 72},
+            "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": res["value"], "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------------- ours ---
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import soi_fft_b200 as sb
+
+    world, rank, local, pg = dist_setup(args)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    N, S = 1 << args.log2n, args.segments
+    # a dedicated stream, handed to the library so its kernels and the timing
+    # events share one stream
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+
+    x128 = make_signal(N, 1234, dev)
+    x32 = x128.to(torch.complex64)
+
+    def new_desc(prec):
+        d = sb.SoiDescriptor(N=N, precision=prec, device=local, stream=stream.cuda_stream)
+        d.init(S)
+        return d
+
+    def barrier():
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize(dev)
+
+    def max_over_ranks(v):
+        if not pg:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(d, src, dst, steps, warmup, per_stage=False):
+        for _ in range(warmup):
+            d.compute_into(src, dst)
+        if per_stage:
+            d.set_timing(True)
+        st = []
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            d.compute_into(src, dst)
+            if per_stage:
+                st.append(d.timings())
+        e1.record(stream)
+        barrier()
+        d.set_timing(False)
+        return e0.elapsed_time(e1), st
+
+    # ---- split precision, device-resident (the headline `value`)
+    d32 = new_desc(sb.PRECISION_SPLIT_FP32)
+    y32 = torch.empty_like(x32)
+    peaks = measured_peaks()
+    with ClockSampler(local) as clk:
+        ms, _ = timed(d32, x32, y32, args.steps, args.warmup)
+    clocks = clk.summary()
+    ms = max_over_ranks(ms)
+    ms_step = ms / args.steps
+    value = world * flop(N) * args.steps / (ms / 1e3) / 1e9
+
+    # per-kernel timing (events recorded by the library on the same stream)
+    _, st = timed(d32, x32, y32, max(2, args.steps // 2), 0, per_stage=True)
+    stage1 = statistics.mean(s["stage1_ms"] for s in st)
+    stage2 = statistics.mean(s["stage2_ms"] for s in st)
+
+    # ---- accuracy vs the FP64 direct FFT (cuFFT Z2Z, checker only)
+    X = torch.fft.fft(x128)
+    nX = torch.linalg.norm(X)
+    acc32 = {"rel_l2": float(torch.linalg.norm(y32.to(torch.complex128) - X) / nX),
+             "max_err": float(torch.sqrt(torch.max((y32.to(torch.complex128) - X).abs() ** 2) /
+                                         torch.max(X.abs() ** 2)))}
+
+    # ---- end to end through the C ABI with pinned host buffers
+    h_in = torch.empty(N, dtype=torch.complex64, pin_memory=True)
+    h_in.copy_(x32)
+    h_out = torch.empty(N, dtype=torch.complex64, pin_memory=True)
+    e2e_steps = max(2, min(args.steps, 5))
+    for _ in range(1):
+        d32.compute_into(h_in.numpy(), h_out.numpy())
+    barrier()
+    t0 = time.perf_counter()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        d32.compute_into(h_in.numpy(), h_out.numpy())
+    e1.record(stream)
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps)
+    e2e_value = world * flop(N) / (e2e_ms / 1e3) / 1e9
+    d32.free()
+    del h_in, h_out
+
+    # ---- plain FP64 method at the same N
+    fp64 = None
+    if not args.no_fp64:
+        d64 = new_desc(sb.PRECISION_FP64)
+        y64 = torch.empty_like(x128)
+        ms64, _ = timed(d64, x128, y64, max(2, min(args.steps, 5)), 2)
+        ms64 = max_over_ranks(ms64) / max(2, min(args.steps, 5))
+        acc64 = float(torch.linalg.norm(y64 - X) / nX)
+        fp64 = {"value": world * flop(N) / (ms64 / 1e3) / 1e9, "unit": "GFLOP/s", "ms_per_step": ms64,
+                "rel_l2_vs_fp64_direct_fft": acc64}
+        d64.free()
+        del y64
+
+    # ---- roofline of the dominant kernel
+    geom = sb.plan_geometry(N, S, sb.PRECISION_SPLIT_FP32)
+    alg_bytes = (N + geom["M_hat"] * S) * 8        # read input, write transposed data
+    hbm = peaks["hbm_gbs"] if peaks else 6650.0
+    achieved = alg_bytes / (stage1 / 1e3) / 1e9
+    roofline = {"kernel": "k_conv_sfft (stage 1: convolution + S-point FFTs + transposed store)",
+                "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_source": "measured" if peaks else "fallback",
+                "traffic": None, "algorithmic_bytes_per_launch": alg_bytes,
+                "stage1_ms": stage1, "stage2_ms": stage2,
+                "pipeline_achieved_gbs": (2 + 2 * 1.25) * N * 8 / (ms_step / 1e3) / 1e9}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline(min(args.log2n, CPU_SAMPLE_LOG2N), S, 2)
+        except Exception as e:  # the checker failing must not hide the measurement
+            cpu = {"error": str(e)[:200]}
+        if cpu and "value" in cpu:
+            cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic: seeded complex Gaussian + 64 tones, amplitudes log-uniform [1e-6, 1]",
+                "config": {"workload": "SOI FFT split-precision, N=2^%d complex64, S=%d, mu=5/4, B=72"
+                                       % (args.log2n, S),
+                           "N": N, "S": S, "mu": "5/4", "B": 72, "precision": "split_fp32",
+                           "l2": "inputs (%d MiB) larger than L2 (126 MB), no flush" % (N * 8 >> 20),
+                           "parallelism": "replicas x%d" % world},
+                "accuracy_vs_fp64_direct_fft": acc32,
+                "fp64_plain": fp64,
+                "split_over_fp64": (value / fp64["value"]) if fp64 else None,
+                "roofline": roofline,
+                "cpu_baseline": cpu,
+                "e2e": {"value": e2e_value, "unit": "GFLOP/s", "ms_per_step": e2e_ms,
+                        "h2d_bytes_per_step": N * 8, "d2h_bytes_per_step": N * 8},
+                "gpu_launches": 3 * args.steps,
+                "clocks": clocks}
+        print(json.dumps(line))
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

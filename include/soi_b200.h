@@ -97,6 +97,10 @@ void parallel_filter_subsampling(soi_desc_t *desc, void *alpha_dt);
 /* ---- status-returning variants ---------------------------------------- */
 int soi_init_status(soi_desc_t *desc, soi_comm_t comm, cfft_size_t k);
 int soi_compute_status(soi_desc_t *desc, void *alpha_dt);
+/* Out-of-place compute_soi: `in` (N inputs) is left untouched, `out`
+ * receives the N outputs; both host or both device memory per device_ptr.
+ * No counterpart in the reference, whose compute_soi is in-place only. */
+int soi_compute_oop_status(soi_desc_t *desc, const void *in, void *out);
 int soi_filter_subsampling_status(soi_desc_t *desc, void *alpha_dt);
 int soi_free_status(soi_desc_t *desc);
 const char *soi_status_string(int status);

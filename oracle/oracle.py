@@ -132,7 +132,7 @@ def ref_available():
 
 
 def run_reference(x, P, k, threads=None, repeat=1, n_mu=5, d_mu=4, B=72, tau=None, sigma=None,
-                  vlc=False):
+                  vlc=False, return_times=False):
     """Run the reference's own compute_soi on P forked ranks x `threads` OpenMP
     threads each.  Returns (output complex128 natural order, best seconds)."""
     x = np.ascontiguousarray(x, dtype=np.complex128)
@@ -158,10 +158,11 @@ def run_reference(x, P, k, threads=None, repeat=1, n_mu=5, d_mu=4, B=72, tau=Non
             raise RuntimeError("reference run failed: %s" % r.stderr[-500:])
         line = [l for l in r.stdout.splitlines() if l.startswith("SOI_REF_RESULT")][-1]
         best = float(line.split("best_s=")[1].split()[0])
+        times = [float(t) for t in line.split("times=")[1].split(",") if t]
         y = np.fromfile(fout, dtype=np.complex128)
     finally:
         for f in (fin, fout):
             if os.path.exists(f):
                 os.remove(f)
         os.rmdir(d)
-    return y, best
+    return (y, best, times) if return_times else (y, best)

@@ -61,6 +61,7 @@ def lib():
             getattr(L, name).argtypes = [P, ctypes.c_void_p, ctypes.c_size_t]
         for name in ("soi_compute_status", "soi_filter_subsampling_status", "soi_get_transposed"):
             getattr(L, name).argtypes = [P, ctypes.c_void_p]
+        L.soi_compute_oop_status.argtypes = [P, ctypes.c_void_p, ctypes.c_void_p]
         L.soi_free_status.argtypes = [P]
         L.set_default_soi_descriptor.argtypes = [P]
         L.soi_status_string.restype = ctypes.c_char_p
@@ -169,6 +170,17 @@ class SoiDescriptor:
         """compute_soi (pfft.c:276-721): in-place; returns x."""
         _check(lib().soi_compute_status(ctypes.byref(self._d), self._ptr(x)), "compute_soi")
         return x
+
+    def compute_into(self, x, out):
+        """Out-of-place transform: x is left untouched, out receives the
+        result (both host arrays or both CUDA tensors)."""
+        px = self._ptr(x)
+        dev = self._d.device_ptr
+        po = self._ptr(out)
+        if self._d.device_ptr != dev:
+            raise ValueError("x and out must both be host arrays or both CUDA tensors")
+        _check(lib().soi_compute_oop_status(ctypes.byref(self._d), px, po), "soi_compute_oop")
+        return out
 
     def filter_subsampling(self, x):
         """parallel_filter_subsampling (.cpp:535): stage 1 only; returns the

@@ -415,22 +415,26 @@ int init_plan(soi_desc_t *d, size_t k)
 
 Plan *plan_of(soi_desc_t *d) { return d ? (Plan *)d->plan : nullptr; }
 
-int compute_impl(soi_desc_t *d, void *alpha, bool stage1_only)
+// One transform: in -> out (they may alias, the reference's in-place form).
+// Host pointers are staged through the plan's device buffer.
+int compute_impl(soi_desc_t *d, const void *in, void *out, bool stage1_only)
 {
   Plan *p = plan_of(d);
   if (!p) return SOI_ERR_NOT_INITIALISED;
   if (cudaSetDevice(p->device) != cudaSuccess) return SOI_ERR_CUDA;
   cudaStream_t st = p->stream;
   const size_t bytes = p->N * p->elem;
-  void *io = alpha;
+  const void *src = in;
+  void *dst = out;
   if (!d->device_ptr) {
     if (!p->d_io) CK(cudaMalloc(&p->d_io, bytes));
-    io = p->d_io;
-    CK(cudaMemcpyAsync(io, alpha, bytes, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(p->d_io, in, bytes, cudaMemcpyHostToDevice, st));
+    src = p->d_io;
+    dst = p->d_io;
   }
   int rc;
   if (p->timing) CK(cudaEventRecord(p->ev[0], st));
-  if ((rc = run_stage1(*p, io, p->d_T, st))) return rc;
+  if ((rc = run_stage1(*p, src, p->d_T, st))) return rc;
   if (p->timing) CK(cudaEventRecord(p->ev[1], st));
   if (stage1_only) {
     CK(cudaStreamSynchronize(st));
@@ -438,9 +442,9 @@ int compute_impl(soi_desc_t *d, void *alpha, bool stage1_only)
   }
   if (d->use_vlc && (rc = run_vlc(*p, p->d_T, st))) return rc;
   if (p->timing) CK(cudaEventRecord(p->ev[2], st));
-  if ((rc = run_stage2(*p, p->d_T, io, st))) return rc;
+  if ((rc = run_stage2(*p, p->d_T, dst, st))) return rc;
   if (p->timing) CK(cudaEventRecord(p->ev[3], st));
-  if (!d->device_ptr) CK(cudaMemcpyAsync(alpha, io, bytes, cudaMemcpyDeviceToHost, st));
+  if (!d->device_ptr) CK(cudaMemcpyAsync(out, p->d_io, bytes, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   if (p->timing) {
     cudaEventElapsedTime(&p->ms[0], p->ev[0], p->ev[1]);
@@ -558,17 +562,25 @@ void init_soi_descriptor(soi_desc_t *d, soi_comm_t comm, cfft_size_t k)
 int soi_compute_status(soi_desc_t *d, void *alpha)
 {
   if (!d) return SOI_ERR_INVALID;
-  int rc = alpha ? compute_impl(d, alpha, false) : SOI_ERR_INVALID;
+  int rc = alpha ? compute_impl(d, alpha, alpha, false) : SOI_ERR_INVALID;
   d->last_status = rc;
   return rc;
 }
 
 void compute_soi(soi_desc_t *d, void *alpha) { die_on(soi_compute_status(d, alpha), "compute_soi"); }
 
+int soi_compute_oop_status(soi_desc_t *d, const void *in, void *out)
+{
+  if (!d) return SOI_ERR_INVALID;
+  int rc = (in && out) ? compute_impl(d, in, out, false) : SOI_ERR_INVALID;
+  d->last_status = rc;
+  return rc;
+}
+
 int soi_filter_subsampling_status(soi_desc_t *d, void *alpha)
 {
   if (!d) return SOI_ERR_INVALID;
-  int rc = alpha ? compute_impl(d, alpha, true) : SOI_ERR_INVALID;
+  int rc = alpha ? compute_impl(d, alpha, alpha, true) : SOI_ERR_INVALID;
   d->last_status = rc;
   return rc;
 }

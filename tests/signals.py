@@ -31,3 +31,22 @@ def band_limited(N, seed, frac=0.05, dtype=np.complex128):
     idx = (k0 + np.arange(W)) % N
     X[idx] = r.standard_normal(W) + 1j * r.standard_normal(W)
     return np.fft.ifft(X).astype(dtype) * np.sqrt(N)
+
+
+def gaussian_plus_tones_torch(N, seed, device="cuda"):
+    """gaussian_plus_tones built on the GPU in FP64 (same recipe, torch RNG)."""
+    import math
+    import torch
+    g = torch.Generator(device=device).manual_seed(seed)
+    x = torch.complex(torch.randn(N, generator=g, device=device, dtype=torch.float64),
+                      torch.randn(N, generator=g, device=device, dtype=torch.float64))
+    n = torch.arange(N, device=device, dtype=torch.int64)
+    r = np.random.default_rng(seed)
+    for _ in range(64):
+        k0 = int(r.integers(0, N))
+        frac = float(r.random())
+        amp = 10.0 ** r.uniform(-6, 0)
+        ph0 = float(r.uniform(0, 2 * math.pi))
+        ph = (torch.remainder(n * k0, N).to(torch.float64) + frac * n.to(torch.float64)) * (2 * math.pi / N) + ph0
+        x += amp * torch.polar(torch.ones_like(ph), ph)
+    return x

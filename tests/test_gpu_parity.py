@@ -50,6 +50,11 @@ def _kw(n, d, B, tau, sigma):
     return kw
 
 
+def _winv_conditioning(N, S, n, d, B, tau, sigma):
+    kw = _kw(n, d, B, tau, sigma)
+    return float(np.abs(sb.window_tables(N, S, **kw)[2]).max())
+
+
 @pytest.mark.parametrize("case", CASES, ids=lambda c: "N%d_S%d_mu%d-%d_B%d" % c[:5])
 def test_fp64_matches_oracle(case):
     N, S, n, d, B, tau, sigma = case
@@ -57,8 +62,18 @@ def test_fp64_matches_oracle(case):
     kw = _kw(n, d, B, tau, sigma)
     ref = oracle.compute_soi(x, S, **kw)
     y = sb.soi_fft(on_gpu(x), S, **kw).cpu().numpy()
-    assert rel_l2(y, ref) <= FP64_TOL
-    assert max_err(y, ref) <= 10 * FP64_TOL
+    X = np.fft.fft(x)
+    # never less accurate than the reference against the exact DFT
+    assert rel_l2(y, X) <= 1.05 * rel_l2(ref, X) + 1e-14
+    if _winv_conditioning(N, S, n, d, B, tau if tau else 928 / 1024., sigma if sigma else 373.7314) <= 1e3:
+        assert rel_l2(y, ref) <= FP64_TOL
+        assert max_err(y, ref) <= 10 * FP64_TOL
+    else:
+        # Narrow windows (max|W_inv| > 1e3): the reference rounds t in double
+        # when tabulating w (pfft.c:52); W_inv amplifies that ~1e-15 error to
+        # >1e-12 at the segment edges.  The tables here use the exact rational
+        # t, so the difference is the reference's rounding, not ours.
+        assert rel_l2(y, ref) <= 1e-10
 
 
 @pytest.mark.parametrize("case", CASES[:8], ids=lambda c: "N%d_S%d_B%d" % (c[0], c[1], c[4]))
@@ -135,15 +150,14 @@ def test_smallest_and_largest_segment_counts():
 def test_large_sizes_against_cufft(N, S):
     # size-independent checks at sizes the CPU oracle is slow for: the FP64
     # direct FFT is cuFFT's Z2Z (called as a library, as the checker only)
-    x = signals.gaussian_plus_tones(N, N + 1)
-    xd = on_gpu(x)
+    xd = signals.gaussian_plus_tones_torch(N, N + 1)
     X = torch.fft.fft(xd)
     y64 = sb.soi_fft(xd, S)
     assert float(torch.linalg.norm(y64 - X) / torch.linalg.norm(X)) <= FP64_TOL
     y32 = sb.soi_fft(xd.to(torch.complex64), S).to(torch.complex128)
     assert float(torch.linalg.norm(y32 - X) / torch.linalg.norm(X)) <= SPLIT_TOL
     # linearity of the FP64 path: T(a x + b u) = a T(x) + b T(u)
-    u = on_gpu(signals.gaussian(N, 2))
+    u = signals.gaussian_plus_tones_torch(N, 2)
     a, b = 0.3 - 1.1j, 2.0 + 0.5j
     lhs = sb.soi_fft(a * xd + b * u, S)
     rhs = a * y64 + b * sb.soi_fft(u, S)
@@ -158,3 +172,21 @@ def test_timings_reported():
     t = d.timings()
     d.free()
     assert t["stage1_ms"] > 0 and t["stage2_ms"] > 0 and t["total_ms"] >= t["stage1_ms"]
+
+
+@pytest.mark.parametrize("prec", [sb.PRECISION_FP64, sb.PRECISION_SPLIT_FP32])
+def test_out_of_place_leaves_input_and_matches_in_place(prec):
+    N, S = 1 << 18, 32
+    dt = np.complex128 if prec == sb.PRECISION_FP64 else np.complex64
+    x = signals.gaussian(N, 9, dt)
+    d = sb.SoiDescriptor(N=N, precision=prec).init(S)
+    xd = on_gpu(x)
+    out = torch.empty_like(xd)
+    d.compute_into(xd, out)
+    assert np.array_equal(xd.cpu().numpy(), x)
+    inplace = d.compute(on_gpu(x)).cpu().numpy()
+    host_out = np.empty_like(x)
+    d.compute_into(x, host_out)
+    d.free()
+    assert np.array_equal(out.cpu().numpy(), inplace)
+    assert np.array_equal(host_out, inplace)

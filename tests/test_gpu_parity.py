@@ -76,8 +76,15 @@ def test_fp64_matches_oracle(case):
         assert rel_l2(y, ref) <= 1e-10
 
 
-@pytest.mark.parametrize("case", CASES[:8], ids=lambda c: "N%d_S%d_B%d" % (c[0], c[1], c[4]))
+SPLIT_CASES = [c for c in CASES[:8] if c[4] != 44]
+
+
+@pytest.mark.parametrize("case", SPLIT_CASES, ids=lambda c: "N%d_S%d_B%d" % (c[0], c[1], c[4]))
 def test_split_fp32_vs_fp64_direct_fft(case):
+    # The split form's error is about eps32 * max|W_inv|: the demodulation
+    # multiplies by W_inv (pfft.c:653-660), up to 9 for the default window but
+    # 1e4 for B=44/tau=0.5 (pfft.c:121), where FP32 cannot reach 1e-6; those
+    # narrow windows are for the FP64 form only.
     N, S, n, d, B, tau, sigma = case
     x = signals.gaussian_plus_tones(N, 3 * N + S)
     X = np.fft.fft(x)
@@ -131,12 +138,24 @@ def test_edge_inputs():
     assert rel_l2(d.compute(e), np.ones(N, np.complex128)) <= FP64_TOL
     # a pure on-bin tone transforms to a single spike
     k0 = 12345
-    t = np.exp(2j * np.pi * k0 * np.arange(N) / N)
+    t = np.exp(2j * np.pi * ((k0 * np.arange(N)) % N) / N)   # phase reduced exactly
     Y = d.compute(t)
     ref = np.zeros(N, np.complex128)
     ref[k0] = N
     assert rel_l2(Y, ref) <= FP64_TOL
     d.free()
+
+
+def test_split_error_scales_with_window_conditioning():
+    # documents the limit stated above: a narrow window in FP32
+    N, S = 1 << 17, 32
+    x = signals.gaussian(N, 1)
+    X = np.fft.fft(x)
+    kw = dict(B=44, tau=512 / 1024, sigma=121.0936)
+    y = sb.soi_fft(on_gpu(x.astype(np.complex64)), S, **kw).cpu().numpy().astype(np.complex128)
+    cond = float(np.abs(sb.window_tables(N, S, **kw)[2]).max())
+    assert cond > 1e3
+    assert rel_l2(y, X) <= 50 * cond * 6e-8
 
 
 def test_smallest_and_largest_segment_counts():

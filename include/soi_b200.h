@@ -145,6 +145,24 @@ int soi_vlc_compress_device(const double *x_dev, int len, int nchunks, int e_max
 /* compress.c:428-544 for each chunk (len a multiple of 16). */
 int soi_vlc_decompress_device(const int *words_dev, long stride_words, int len, int nchunks,
                               int e_max, const int *e_max_i_dev, double *out_dev, void *stream);
+/* The same round trip (max_exponent, global maximum, compress, decompress)
+ * for callers that cannot call cudaMalloc -- a process whose device memory is
+ * already reserved by its own pool allocator, or a latency-critical loop that
+ * must not pay cudaMalloc/cudaFree's device-wide synchronisation.  No
+ * counterpart in the reference.  It allocates nothing: its scratch is a
+ * static device array of 32 MiB of compressed words (plus 16 KiB of
+ * per-chunk exponents and counts) that every GPU loading this library holds
+ * until the process exits.  Limits: len a multiple of 16, nchunks <= 2047,
+ * nchunks * soi_vlc_words(len, 0, 0) <= 8388608 (about 2.4M doubles in
+ * total); larger requests return SOI_ERR_INVALID with a message on stderr.
+ * The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * All calls share the one array: calls that overlap on the GPU (different
+ * streams, or host threads without ordering) race and corrupt each other.
+ * x_dev: nchunks*len doubles in, out_dev: nchunks*len doubles out, on
+ * `stream`; the call returns without synchronising. */
+int soi_vlc_roundtrip_noalloc_device(const double *x_dev, double *out_dev, int len, int nchunks,
+                                     void *stream);
 /* Words compress() writes for one chunk (pfft.c:397-402 sizing). */
 int soi_vlc_words(int len, int e_max, int e_max_i);
 

@@ -10,6 +10,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <vector>
 
 #include "../../include/soi_b200.h"
@@ -719,3 +720,90 @@ int soi_vlc_decompress_device(const int *words, long stride_words, int len, int 
 }
 
 }  // extern "C"
+
+// ======================================== VLC round trip without allocation ==
+//
+// soi_vlc_roundtrip_noalloc_device: the same max_exponent -> compress ->
+// decompress round trip as the three soi_vlc_*_device entry points, for
+// callers that cannot call cudaMalloc: a host program whose device memory is
+// already handed out to its own pool (a framework's caching allocator that
+// reserves the GPU at start-up), or a latency-critical loop in which the
+// device-wide synchronisation of cudaMalloc/cudaFree is not acceptable.  Its
+// scratch (per-chunk exponents, word counts and the compressed words) lives in
+// the file-scope array below, which every GPU that loads this library holds
+// until the process exits.
+
+namespace {
+
+constexpr long long kNoallocHeaderInts = 4096;              // e_max[<=2047], gmax, nwords[<=2047]
+constexpr long long kNoallocWordInts = 8ll << 20;            // 32 MiB of compressed words
+constexpr int kNoallocMaxChunks = 2047;
+constexpr int kNoallocMaxDevices = 64;
+
+static __device__ __align__(256) int g_noalloc_scratch[kNoallocHeaderInts + kNoallocWordInts];
+
+int *g_noalloc_ptr[kNoallocMaxDevices] = {};
+std::atomic<int> g_noalloc_lock{0};
+
+// Device address of g_noalloc_scratch on the current device, looked up once
+// per device (cudaGetSymbolAddress with that device current) and cached.
+int noalloc_scratch(int **ptr)
+{
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoallocMaxDevices) return SOI_ERR_UNSUPPORTED;
+  while (g_noalloc_lock.exchange(1)) {}
+  int rc = SOI_OK;
+  if (!g_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+      fprintf(stderr, "soi_b200: cudaGetSymbolAddress(g_noalloc_scratch) failed: %s\n", cudaGetErrorString(e));
+      rc = SOI_ERR_CUDA;
+    } else {
+      g_noalloc_ptr[dev] = (int *)p;
+    }
+  }
+  *ptr = g_noalloc_ptr[dev];
+  g_noalloc_lock.store(0);
+  return rc;
+}
+
+}  // namespace
+
+extern "C" int soi_vlc_roundtrip_noalloc_device(const double *x_dev, double *out_dev, int len, int nchunks,
+                                                void *stream)
+{
+  if (!x_dev || !out_dev || len <= 0 || nchunks <= 0) return SOI_ERR_INVALID;
+  if (len % 16) return SOI_ERR_UNSUPPORTED;
+  // worst case of compress(): every element at full width (56 bits)
+  const long long per_chunk = soi_vlc_words(len, 0, 0);
+  if (nchunks > kNoallocMaxChunks || per_chunk * nchunks > kNoallocWordInts) {
+    fprintf(stderr,
+            "soi_vlc_roundtrip_noalloc_device: %d chunks of %d doubles need %lld scratch words; the static "
+            "scratch holds %lld words in at most %d chunks\n",
+            nchunks, len, per_chunk * nchunks, kNoallocWordInts, kNoallocMaxChunks);
+    return SOI_ERR_INVALID;
+  }
+  int *scr = nullptr;
+  int rc = noalloc_scratch(&scr);
+  if (rc) return rc;
+  int *e_max_i = scr;                       // [nchunks]
+  int *g_max = scr + kNoallocMaxChunks;     // [1]
+  int *nwords = scr + kNoallocMaxChunks + 1;
+  int *words = scr + kNoallocHeaderInts;    // [nchunks][per_chunk]
+  cudaStream_t st = (cudaStream_t)stream;
+  // every scratch entry read below is written earlier in this call (exponents,
+  // maximum, counts, and each compressed word including its zero padding), so
+  // nothing has to be cleared first
+  vlc_max_exponent_kernel<<<nchunks, 256, 0, st>>>(x_dev, len, e_max_i);
+  CK(cudaGetLastError());
+  vlc_global_max<<<1, 256, 0, st>>>(e_max_i, nchunks, g_max);
+  CK(cudaGetLastError());
+  dim3 g(64, (unsigned)nchunks);
+  vlc_compress_kernel<<<g, 256, 0, st>>>(x_dev, len, 0, g_max, e_max_i, words, (long)per_chunk, nwords);
+  CK(cudaGetLastError());
+  vlc_decompress_kernel<<<g, 256, 0, st>>>(words, (long)per_chunk, len, nullptr, g_max, e_max_i, out_dev);
+  CK(cudaGetLastError());
+  return SOI_OK;
+}

@@ -166,6 +166,21 @@ int soi_vlc_roundtrip_noalloc_device(const double *x_dev, double *out_dev, int l
 /* Words compress() writes for one chunk (pfft.c:397-402 sizing). */
 int soi_vlc_words(int len, int e_max, int e_max_i);
 
+/* ---- learned window surrogate (no counterpart in the reference) --------- */
+
+/* A 4-64-64-1 GELU MLP (FP32) predicting log10 of the transform's relative L2
+ * error for a window (inputs normalised by soi_fft_b200/window_mlp.py).
+ * Parameters: soi_mlp_param_count() floats, layout W1[64][4] b1 W2[64][64]
+ * b2 W3[64] b3.  All pointers are device pointers. */
+int soi_mlp_param_count(void);
+/* y[i] = MLP(x[i][0..4)) for i < n */
+int soi_mlp_forward_device(const float *params, const float *x, float *y, int n, void *stream);
+/* grad = d/dparams of mean((MLP(x) - y)^2), loss = that mean; both overwritten */
+int soi_mlp_grad_device(const float *params, const float *x, const float *y, int n, float *grad, float *loss,
+                        void *stream);
+/* one Adam step (beta1 0.9, beta2 0.999, eps 1e-8) at 1-based step count */
+int soi_mlp_adam_device(float *params, float *m, float *v, const float *grad, float lr, int step, void *stream);
+
 /* ---- host-side tables (no GPU needed) ---------------------------------- */
 
 /* The factorised window the kernels use: for output phase theta, tap kk and

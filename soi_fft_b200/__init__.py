@@ -82,6 +82,11 @@ def lib():
         L.soi_vlc_decompress_device.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_int, ctypes.c_int,
                                                 ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                                 ctypes.c_void_p]
+        V = ctypes.c_void_p
+        L.soi_mlp_param_count.restype = ctypes.c_int
+        L.soi_mlp_forward_device.argtypes = [V, V, V, ctypes.c_int, V]
+        L.soi_mlp_grad_device.argtypes = [V, V, V, ctypes.c_int, V, V, V]
+        L.soi_mlp_adam_device.argtypes = [V, V, V, V, ctypes.c_float, ctypes.c_int, V]
         _lib = L
     return _lib
 

@@ -1,0 +1,138 @@
+// fft_reg.cuh -- register-resident DFTs of compile-time size F <= 64 built
+// from the radix-2/3/4/5/8 butterflies, with twiddles in constant memory.
+//
+// RegDFT<V, F>::run(v) transforms v[0..F) in place, natural order in and out,
+// forward (exp(-2 pi i jk/F)).  F = A*Bq is split as a four-step in
+// registers: A-point DFTs over the stride-Bq subsequences, twiddles
+// w_F^(b*ka), Bq-point DFTs, then a compile-time permutation (register
+// renaming, no data movement after unrolling).
+#pragma once
+
+#include "fft_device.cuh"
+
+namespace soi {
+
+// sizes with a twiddle table in constant memory, and their offsets
+constexpr int kRegSizes[] = { 2, 3, 4, 5, 6, 8, 10, 12, 15, 16, 20, 24, 30, 32, 40, 48, 60, 64 };
+__host__ __device__ constexpr int reg_tw_offset(int F)
+{
+  // cumulative sizes of kRegSizes (a table lookup is not usable in device code)
+  return F == 2 ? 0 : F == 3 ? 2 : F == 4 ? 5 : F == 5 ? 9 : F == 6 ? 14 : F == 8 ? 20 : F == 10 ? 28
+       : F == 12 ? 38 : F == 15 ? 50 : F == 16 ? 65 : F == 20 ? 81 : F == 24 ? 101 : F == 30 ? 125
+       : F == 32 ? 155 : F == 40 ? 187 : F == 48 ? 227 : F == 60 ? 275 : F == 64 ? 335 : -1;
+}
+constexpr int kRegTwTotal = 399;
+
+// w_F^m = exp(-2 pi i m/F) at c_regtw[reg_tw_offset(F) + m]; filled by the
+// host (long double, rounded once) before the first launch.
+__constant__ float2 c_regtw_f[kRegTwTotal];
+__constant__ double2 c_regtw_d[kRegTwTotal];
+
+template <typename V> __device__ __forceinline__ V regtw(int idx);
+template <> __device__ __forceinline__ float2 regtw<float2>(int idx) { return c_regtw_f[idx]; }
+template <> __device__ __forceinline__ double2 regtw<double2>(int idx) { return c_regtw_d[idx]; }
+
+template <int F> struct RegSplit {
+  // sizes with a direct butterfly are not split
+  static constexpr int A = (F == 2 || F == 3 || F == 4 || F == 5 || F == 8) ? F
+                         : (F % 8 == 0 && F > 8) ? 8
+                         : (F % 4 == 0 && F > 4) ? 4
+                         : (F % 2 == 0 && F > 2) ? 2
+                         : (F % 5 == 0 && F > 5) ? 5
+                         : (F % 3 == 0 && F > 3) ? 3 : F;
+};
+
+template <typename V, int F> struct RegDFT {
+  static __device__ __forceinline__ void run(V *v)
+  {
+    constexpr int A = RegSplit<F>::A;
+    constexpr int Bq = F / A;
+    if constexpr (Bq == 1) {
+      Bfly<V, F>::run(v, nullptr);
+    } else {
+      constexpr int off = reg_tw_offset(F);
+      static_assert(off >= 0, "register DFT size without a twiddle table");
+#pragma unroll
+      for (int b = 0; b < Bq; ++b) {
+        V u[A];
+#pragma unroll
+        for (int a = 0; a < A; ++a) u[a] = v[b + Bq * a];
+        Bfly<V, A>::run(u, nullptr);
+#pragma unroll
+        for (int a = 0; a < A; ++a) v[b + Bq * a] = (b * a == 0) ? u[a] : cmul(u[a], regtw<V>(off + b * a));
+      }
+      // for each ka the Bq values v[b + Bq*ka] are contiguous: transform them
+#pragma unroll
+      for (int a = 0; a < A; ++a) RegDFT<V, Bq>::run(v + Bq * a);
+      // v[Bq*ka + kb] = X[ka + A*kb]
+      V t[F];
+#pragma unroll
+      for (int ka = 0; ka < A; ++ka)
+#pragma unroll
+        for (int kb = 0; kb < Bq; ++kb) t[ka + A * kb] = v[Bq * ka + kb];
+#pragma unroll
+      for (int i = 0; i < F; ++i) v[i] = t[i];
+    }
+  }
+};
+
+// In-place tile FFT on a shared-memory tile already holding the input (the
+// caller prefetched it with cp.async).  Radices R0, R1, R2 (R2 = 1: two
+// stages).  Shared index of (col, pos): (pos + pos/RL)*PP + col*PC with RL the
+// last radix (one pad element per last-stage group).  The last stage hands each
+// thread RL outputs of one column in frequency order f = fbase + (L/RL)*k to
+// `emit`, which loads its epilogue factors before storing.
+template <typename V, int R0, int R1, int R2, class Emit>
+__device__ __forceinline__ void tile_fft_smem(V *sm, int C, int PP, int PC, const V *__restrict__ tw,
+                                              const Emit &emit)
+{
+  constexpr int RL = (R2 > 1) ? R2 : R1;
+  constexpr int L = R0 * R1 * R2;
+  constexpr int span0 = L / R0;
+  auto sidx = [&](int col, int pos) { return (pos + pos / RL) * PP + col * PC; };
+  {
+    const int n = C * span0;
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+      const int col = q % C, i = q / C;
+      V v[R0];
+#pragma unroll
+      for (int r = 0; r < R0; ++r) v[r] = sm[sidx(col, i + r * span0)];
+      RegDFT<V, R0>::run(v);
+#pragma unroll
+      for (int k = 0; k < R0; ++k) sm[sidx(col, i + k * span0)] = (k && i) ? cmul(v[k], tw[i * k]) : v[k];
+    }
+  }
+  __syncthreads();
+  if constexpr (R2 > 1) {
+    constexpr int span1 = span0 / R1;
+    const int n = C * (L / R1);
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+      const int col = q % C, t = q / C;
+      const int blk = t / span1, i = t - blk * span1;
+      const int base = blk * span0 + i;
+      V v[R1];
+#pragma unroll
+      for (int r = 0; r < R1; ++r) v[r] = sm[sidx(col, base + r * span1)];
+      RegDFT<V, R1>::run(v);
+#pragma unroll
+      for (int k = 0; k < R1; ++k) sm[sidx(col, base + k * span1)] = (k && i) ? cmul(v[k], tw[i * k * R0]) : v[k];
+    }
+    __syncthreads();
+  }
+  {
+    const int n = C * (L / RL);
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+      const int col = q % C, blk = q / C;
+      V v[RL];
+#pragma unroll
+      for (int r = 0; r < RL; ++r) v[r] = sm[sidx(col, blk * RL + r)];
+      RegDFT<V, RL>::run(v);
+      int fbase;
+      if constexpr (R2 > 1) fbase = (blk / R1) + R0 * (blk % R1);
+      else fbase = blk;
+      emit.template run<RL>(col, fbase, L / RL, v);
+    }
+  }
+}
+
+}  // namespace soi

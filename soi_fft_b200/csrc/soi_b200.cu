@@ -16,6 +16,9 @@
 #include "../../include/soi_b200.h"
 #include "soi_kernels.cuh"
 #include "vlc_kernels.cuh"
+#include "stage2_fast.cuh"
+#include "stage1_fast.cuh"
+#include "mlp_kernels.cuh"
 
 using namespace soi;
 
@@ -46,6 +49,23 @@ struct Plan {
   double *d_vlc_x = nullptr;   // promoted/decompressed doubles (FP32 path)
   int *d_vlc_words = nullptr, *d_vlc_n = nullptr, *d_vlc_emax = nullptr;
   long vlc_stride = 0;
+  // persistent stage 2 (split form): compiled radix split and its state
+  int fast2 = 0;               // 0: two-kernel stage 2, 1: persistent kernel
+  int f2_variant = 0;
+  int f2_grid = 0;
+  size_t f2_smem = 0;
+  int f2_ps2 = 0;
+  int f2_buf = 0;
+  void *d_amp = nullptr;            // [M/2+1] real demodulation amplitude
+  double2 *d_dlo = nullptr, *d_dhi = nullptr;
+  int dlo_bits = 11;
+  void (*f2_kernel)(S2Args) = nullptr;
+  unsigned int *d_sync = nullptr;   // [0] counter, [1] err, [2..2+S) done1
+  // staged stage 1
+  int s1fast = 0, JR2 = 0, JT2 = 0, AC = 0, buf_elems = 0;
+  int s1_tS = 0;                    // compile-time-S stage-1 instance available
+  size_t smem1b = 0;
+  void *d_filt2 = nullptr;          // [d][atap][nmu][S] real
   bool timing = false;
   cudaEvent_t ev[5] = {};
   float ms[4] = {0, 0, 0, 0};
@@ -59,6 +79,12 @@ struct Plan {
       return SOI_ERR_CUDA;                                                       \
     }                                                                            \
   } while (0)
+
+int env_int(const char *name, int dflt)
+{
+  const char *v = getenv(name);
+  return v ? atoi(v) : dflt;
+}
 
 // ---- FFT planning ------------------------------------------------------------
 
@@ -240,14 +266,272 @@ int launch_seg_t(Plan &p, void *T, void *out, cudaStream_t st)
   return SOI_OK;
 }
 
+// ---- persistent stage 2 -------------------------------------------------------
+
+using S2Kernel = void (*)(S2Args);
+
+struct S2Choice { int M1, M2, r0, r1, r2, q0, q1, q2; S2Kernel k; };
+
+// compiled splits (split form): M1 = r0*r1*r2, M2 = q0*q1*q2
+const S2Choice kS2Choices[] = {
+  { 2560, 2048, 10, 16, 16, 8, 16, 16, k_stage2_persistent<float, 10, 16, 16, 8, 16, 16> },
+  { 2560, 2048, 40, 64, 1, 32, 64, 1, k_stage2_persistent<float, 40, 64, 1, 32, 64, 1> },
+  { 2560, 1024, 10, 16, 16, 4, 16, 16, k_stage2_persistent<float, 10, 16, 16, 4, 16, 16> },
+  { 1280, 1024, 5, 16, 16, 4, 16, 16, k_stage2_persistent<float, 5, 16, 16, 4, 16, 16> },
+  { 1280, 512, 5, 16, 16, 8, 8, 8, k_stage2_persistent<float, 5, 16, 16, 8, 8, 8> },
+  { 640, 1024, 10, 8, 8, 4, 16, 16, k_stage2_persistent<float, 10, 8, 8, 4, 16, 16> },
+  { 640, 512, 10, 8, 8, 8, 8, 8, k_stage2_persistent<float, 10, 8, 8, 8, 8, 8> },
+  { 320, 512, 5, 8, 8, 8, 8, 8, k_stage2_persistent<float, 5, 8, 8, 8, 8, 8> },
+  { 320, 256, 5, 8, 8, 4, 8, 8, k_stage2_persistent<float, 5, 8, 8, 4, 8, 8> },
+};
+
+// Select a compiled persistent split for M' (split form only); returns the
+// index into kS2Choices or -1.  Three-stage register splits are preferred;
+// SOI_STAGE2_VARIANT=2 selects the two-stage (radix-64) one where compiled.
+int pick_fast2(const Plan &p)
+{
+  if (p.prec != SOI_PRECISION_SPLIT_FP32 || env_int("SOI_STAGE2_FAST", 1) == 0) return -1;
+  const bool want2 = env_int("SOI_STAGE2_VARIANT", 0) == 2;
+  int best = -1;
+  for (int i = 0; i < (int)(sizeof(kS2Choices) / sizeof(kS2Choices[0])); ++i) {
+    const S2Choice &c = kS2Choices[i];
+    if ((long long)c.M1 * c.M2 != (long long)p.Mh) continue;
+    const bool two = c.r2 == 1;
+    if (best < 0 || (two == want2 && (kS2Choices[best].r2 == 1) != want2)) best = i;
+  }
+  return best;
+}
+
+// Register-DFT twiddles in constant memory (long double, rounded once).
+// Every kernel built on RegDFT reads them, so every plan uploads them to its
+// device.
+int upload_regtw()
+{
+  std::vector<float2> tf(kRegTwTotal);
+  std::vector<double2> td(kRegTwTotal);
+  for (int F : kRegSizes) {
+    const int off = reg_tw_offset(F);
+    for (int m = 0; m < F; ++m) {
+      long double ang = -2.0L * kPi * (long double)m / (long double)F;
+      tf[off + m] = make_float2((float)cosl(ang), (float)sinl(ang));
+      td[off + m] = make_double2((double)cosl(ang), (double)sinl(ang));
+    }
+  }
+  CK(cudaMemcpyToSymbol(c_regtw_f, tf.data(), tf.size() * sizeof(float2)));
+  CK(cudaMemcpyToSymbol(c_regtw_d, td.data(), td.size() * sizeof(double2)));
+  return SOI_OK;
+}
+
+int setup_fast2(Plan &p, int idx)
+{
+  const S2Choice &c = kS2Choices[idx];
+  p.M1 = c.M1; p.M2 = c.M2;
+  p.C1 = 2; p.C2 = 2;                      // 16-byte column runs; neighbouring tiles share sectors in L2
+  const int RLa = c.r2 > 1 ? c.r2 : c.r1, RLb = c.q2 > 1 ? c.q2 : c.q1;
+  const size_t smA = (size_t)(p.M1 + p.M1 / RLa) * p.C1;
+  int ps2 = p.M2 + p.M2 / RLb;
+  while (ps2 % 16 != 8) ++ps2;             // pass-2 columns 16 words apart in the banks
+  p.f2_ps2 = ps2;
+  const size_t smB = (size_t)ps2 * p.C2;
+  size_t be = std::max(smA, smB);
+  be += be & 1;
+  p.f2_buf = (int)be;
+  p.f2_smem = be * p.elem;
+  p.f2_kernel = c.k;
+  CK(cudaFuncSetAttribute(c.k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.f2_smem));
+  int occ = 0, nsm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, c.k, 128, p.f2_smem));
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, p.device));
+  if (occ < 1) return SOI_ERR_UNSUPPORTED;
+  p.f2_grid = occ * nsm;
+  CK(cudaMalloc(&p.d_sync, (p.S + 2) * sizeof(unsigned int)));
+  // demodulation W_inv[k] = exp(-i pi kappa k/M) * amp[k] (pfft.c:68-82):
+  // amp = 1/y_W(k/M - 1/2) is even about M/2, kept for k <= M/2 and rounded
+  // once; the phase is formed in FP64 from two tables
+  {
+    const size_t M = p.M, half = M / 2 + 1;
+    const long double sq = sqrtl((long double)p.sigma);
+    std::vector<float> af(half);
+    for (size_t i = 0; i < half; ++i) {
+      long double t = (long double)i / (long double)M - 0.5L;
+      long double y = (erfcl(sq * (t - p.tau / 2.0L)) - erfcl(sq * (t + p.tau / 2.0L))) / (2.0L * p.tau);
+      af[i] = (float)(1.0L / y);
+    }
+    int rc;
+    if ((rc = upload(&p.d_amp, af.data(), af.size() * sizeof(float)))) return rc;
+    const long long kappa = (long long)p.B - p.dmu;
+    const long long nlo = 1LL << p.dlo_bits, nhi = (long long)(M >> p.dlo_bits) + 2;
+    std::vector<double> lo(2 * nlo), hi(2 * nhi);
+    auto phase = [&](long long k, double *o) {
+      long long q = (long long)(((unsigned long long)kappa * (unsigned long long)k) % (2ULL * M));
+      long double ang = -kPi * (long double)q / (long double)M;
+      o[0] = (double)cosl(ang);
+      o[1] = (double)sinl(ang);
+    };
+    for (long long e = 0; e < nlo; ++e) phase(e, &lo[2 * e]);
+    for (long long h = 0; h < nhi; ++h) phase(h * nlo, &hi[2 * h]);
+    if ((rc = upload((void **)&p.d_dlo, lo.data(), lo.size() * sizeof(double)))) return rc;
+    if ((rc = upload((void **)&p.d_dhi, hi.data(), hi.size() * sizeof(double)))) return rc;
+  }
+  p.fast2 = 1;
+  return SOI_OK;
+}
+
+int launch_fast2(Plan &p, void *T, void *out, cudaStream_t st)
+{
+  S2Args a;
+  a.T = T; a.out = out; a.tw1 = p.d_tw1; a.tw2 = p.d_tw2; a.xlo = p.d_xlo; a.xhi = p.d_xhi;
+  a.winv = p.d_winv; a.Mh = (long long)p.Mh; a.M = (long long)p.M;
+  a.M1 = p.M1; a.M2 = p.M2; a.C1 = p.C1; a.C2 = p.C2; a.S = (int)p.S; a.lo_bits = p.lo_bits;
+  a.nt1 = p.M2 / p.C1; a.nt2 = p.M1 / p.C2; a.ps2 = p.f2_ps2;
+  a.discard = env_int("SOI_STAGE2_DISCARD", 1);
+  a.amp = p.d_amp; a.dlo = p.d_dlo; a.dhi = p.d_dhi; a.dlo_bits = p.dlo_bits; a.buf_elems = p.f2_buf;
+  a.counter = p.d_sync; a.err = (int *)(p.d_sync + 1); a.done1 = p.d_sync + 2;
+  CK(cudaMemsetAsync(p.d_sync, 0, (p.S + 2) * sizeof(unsigned int), st));
+  p.f2_kernel<<<p.f2_grid, 128, p.f2_smem, st>>>(a);
+  CK(cudaGetLastError());
+  return SOI_OK;
+}
+
+int check_fast2(Plan &p, cudaStream_t st)
+{
+  if (!p.fast2) return SOI_OK;
+  int err = 0;
+  CK(cudaMemcpyAsync(&err, p.d_sync + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return err ? SOI_ERR_TIMEOUT : SOI_OK;
+}
+
+template <typename R, int NMU, int JR>
+int launch_conv2_t(Plan &p, const void *alpha, void *T, cudaStream_t st)
+{
+  Conv2Args a;
+  a.alpha = alpha; a.T = T; a.filt = p.d_filt2; a.phase = p.d_phase; a.twS = p.d_twS;
+  a.permS = p.d_permS; a.wsmall = p.d_wsmall; a.planS = p.planS;
+  a.M = (long long)p.M; a.Mh = (long long)p.Mh; a.J = (long long)p.J;
+  a.S = (int)p.S; a.d = p.dmu; a.atap = p.atap; a.JT = p.JT2; a.pitch = p.pitch; a.AC = p.AC;
+  a.buf_elems = p.buf_elems;
+  auto kern = k_conv_sfft_staged<R, NMU, JR>;
+  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem1b));
+  dim3 grid((unsigned)((p.J + p.JT2 - 1) / p.JT2));
+  kern<<<grid, 512, p.smem1b, st>>>(a);
+  CK(cudaGetLastError());
+  return SOI_OK;
+}
+
+// staged stage-1 instances: (precision, n_mu) -> JR
+int staged_jr(int prec, int nmu)
+{
+  if (prec == SOI_PRECISION_SPLIT_FP32) return nmu == 5 ? 6 : nmu == 3 ? 6 : (nmu == 8 || nmu == 9) ? 4 : 0;
+  return nmu == 5 ? 4 : nmu == 3 ? 4 : (nmu == 8 || nmu == 9) ? 2 : 0;
+}
+
+template <typename R, int NMU, int JR, int R0, int R1>
+int launch_conv_tS(Plan &p, const void *alpha, void *T, cudaStream_t st)
+{
+  Conv2Args a;
+  a.alpha = alpha; a.T = T; a.filt = p.d_filt2; a.phase = p.d_phase; a.twS = p.d_twS;
+  a.permS = p.d_permS; a.wsmall = p.d_wsmall; a.planS = p.planS;
+  a.M = (long long)p.M; a.Mh = (long long)p.Mh; a.J = (long long)p.J;
+  a.S = (int)p.S; a.d = p.dmu; a.atap = p.atap; a.JT = p.JT2; a.pitch = p.pitch; a.AC = p.AC;
+  a.buf_elems = p.buf_elems;
+  auto kern = k_conv_sfft_tS<R, NMU, JR, R0, R1>;
+  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem1b));
+  dim3 grid((unsigned)((p.J + p.JT2 - 1) / p.JT2));
+  kern<<<grid, 512, p.smem1b, st>>>(a);
+  CK(cudaGetLastError());
+  return SOI_OK;
+}
+
+// compile-time-S instances: n_mu = 5, S in {8..256} (R0*R1 split of S)
+template <typename R, int JR>
+int launch_tS_switch(Plan &p, const void *alpha, void *T, cudaStream_t st)
+{
+  switch (p.S) {
+    case 8: return launch_conv_tS<R, 5, JR, 2, 4>(p, alpha, T, st);
+    case 16: return launch_conv_tS<R, 5, JR, 4, 4>(p, alpha, T, st);
+    case 32: return launch_conv_tS<R, 5, JR, 4, 8>(p, alpha, T, st);
+    case 64: return launch_conv_tS<R, 5, JR, 8, 8>(p, alpha, T, st);
+    case 128: return launch_conv_tS<R, 5, JR, 8, 16>(p, alpha, T, st);
+    case 256: return launch_conv_tS<R, 5, JR, 16, 16>(p, alpha, T, st);
+  }
+  return SOI_ERR_UNSUPPORTED;
+}
+
+bool tS_available(const Plan &p)
+{
+  if (p.nmu != 5 || env_int("SOI_STAGE1_TS", 1) == 0) return false;
+  return p.S == 8 || p.S == 16 || p.S == 32 || p.S == 64 || p.S == 128 || p.S == 256;
+}
+
+// last radix of the compile-time-S split (the tile layout pads every R1)
+int tS_r1(size_t S) { return S == 8 ? 4 : S == 16 ? 4 : S == 32 ? 8 : S == 64 ? 8 : 16; }
+
+int launch_conv2(Plan &p, const void *alpha, void *T, cudaStream_t st)
+{
+  if (p.s1_tS)
+    return p.prec == SOI_PRECISION_SPLIT_FP32 ? launch_tS_switch<float, 6>(p, alpha, T, st)
+                                              : launch_tS_switch<double, 4>(p, alpha, T, st);
+  if (p.prec == SOI_PRECISION_SPLIT_FP32) {
+    switch (p.nmu) {
+      case 5: return launch_conv2_t<float, 5, 6>(p, alpha, T, st);
+      case 3: return launch_conv2_t<float, 3, 6>(p, alpha, T, st);
+      case 8: return launch_conv2_t<float, 8, 4>(p, alpha, T, st);
+      case 9: return launch_conv2_t<float, 9, 4>(p, alpha, T, st);
+    }
+  } else {
+    switch (p.nmu) {
+      case 5: return launch_conv2_t<double, 5, 4>(p, alpha, T, st);
+      case 3: return launch_conv2_t<double, 3, 4>(p, alpha, T, st);
+      case 8: return launch_conv2_t<double, 8, 2>(p, alpha, T, st);
+      case 9: return launch_conv2_t<double, 9, 2>(p, alpha, T, st);
+    }
+  }
+  return SOI_ERR_UNSUPPORTED;
+}
+
+// tile geometry of the staged kernel; leaves s1fast = 0 when it does not apply
+void plan_stage1_staged(Plan &p)
+{
+  p.s1fast = 0;
+  if (env_int("SOI_STAGE1_FAST", 1) == 0) return;
+  const int jr = staged_jr(p.prec, p.nmu);
+  if (!jr || p.S > 512 || (p.S * p.nmu) % 4) return;
+  const int groups = 512 / (int)p.S;
+  const size_t budget = 200 * 1024 - p.S * (p.elem + sizeof(int));
+  const size_t real = p.elem / 2;
+  const bool ts = tS_available(p);
+  const size_t pitch = ts ? ((p.S + p.S / tS_r1(p.S)) | 1) : (size_t)p.pitch;
+  for (int jt = groups * jr; jt >= jr; jt -= jr) {
+    if ((long long)jt > (long long)p.J - p.atap - jt) continue;     // keep the wrap single-step
+    for (int ac = p.atap; ac >= 1; --ac) {
+      const size_t rows = (size_t)(jt + ac - 1) * p.S;
+      const size_t fel = ((size_t)ac * p.nmu * p.S * real + p.elem - 1) / p.elem;
+      size_t be = rows + fel;
+      const size_t tile = (size_t)p.nmu * jt * pitch;
+      be = std::max(be, (tile + 1) / 2);
+      be = (be * p.elem + 15) / 16 * 16 / p.elem;   // both buffers start on 16-byte boundaries (cp.async 16)
+      if (2 * be * p.elem <= budget) {
+        p.JR2 = jr; p.JT2 = jt; p.AC = ac; p.buf_elems = (int)be;
+        p.smem1b = 2 * be * p.elem + p.S * (p.elem + sizeof(int));
+        p.s1fast = 1;
+        p.s1_tS = ts ? 1 : 0;
+        return;
+      }
+    }
+  }
+}
+
 int run_stage1(Plan &p, const void *alpha, void *T, cudaStream_t st)
 {
+  if (p.s1fast) return launch_conv2(p, alpha, T, st);
   return p.prec == SOI_PRECISION_FP64 ? launch_conv_r<double>(p, alpha, T, st)
                                       : launch_conv_r<float>(p, alpha, T, st);
 }
 
 int run_stage2(Plan &p, void *T, void *out, cudaStream_t st)
 {
+  if (p.fast2) return launch_fast2(p, T, out, st);
   return p.prec == SOI_PRECISION_FP64 ? launch_seg_t<double>(p, T, out, st)
                                       : launch_seg_t<float>(p, T, out, st);
 }
@@ -319,6 +603,18 @@ int build_tables(Plan &p)
   round_complex<R>(wir, wii, wi);
   int rc;
   if ((rc = upload(&p.d_filt, f.data(), f.size() * sizeof(R)))) return rc;
+  if (p.s1fast) {
+    // branch-major copy for the staged kernel: [b][a][theta][s] = filt[d*a + b][theta][s]
+    std::vector<R> f2((size_t)p.dmu * p.atap * p.nmu * p.S, (R)0);
+    for (int b = 0; b < p.dmu; ++b)
+      for (int aa = 0; aa < p.atap; ++aa) {
+        const size_t kk = (size_t)p.dmu * aa + b;
+        for (int th = 0; th < p.nmu; ++th)
+          for (size_t sc = 0; sc < p.S; ++sc)
+            f2[(((size_t)b * p.atap + aa) * p.nmu + th) * p.S + sc] = f[(kk * p.nmu + th) * p.S + sc];
+      }
+    if ((rc = upload(&p.d_filt2, f2.data(), f2.size() * sizeof(R)))) return rc;
+  }
   if ((rc = upload(&p.d_phase, ph.data(), ph.size() * sizeof(R)))) return rc;
   if ((rc = upload(&p.d_winv, wi.data(), wi.size() * sizeof(R)))) return rc;
   std::vector<R> tS = roots_table<R>((long long)p.S), t1 = roots_table<R>(p.M1), t2 = roots_table<R>(p.M2);
@@ -356,7 +652,7 @@ void free_plan(Plan *p)
   cudaSetDevice(p->device);
   void *bufs[] = { p->d_filt, p->d_phase, p->d_twS, p->d_tw1, p->d_tw2, p->d_winv, p->d_wsmall,
                    p->d_permS, p->d_perm1, p->d_perm2, p->d_xlo, p->d_xhi, p->d_T, p->d_io,
-                   p->d_vlc_x, p->d_vlc_words, p->d_vlc_n, p->d_vlc_emax };
+                   p->d_vlc_x, p->d_vlc_words, p->d_vlc_n, p->d_vlc_emax, p->d_sync, p->d_filt2, p->d_amp, p->d_dlo, p->d_dhi };
   for (void *b : bufs) if (b) cudaFree(b);
   for (auto &e : p->ev) if (e) cudaEventDestroy(e);
   if (p->own_stream && p->stream) cudaStreamDestroy(p->stream);
@@ -389,6 +685,18 @@ int plan_geometry(const soi_desc_t *d, size_t k, Plan &p)
   if (jt < p.JR) return SOI_ERR_UNSUPPORTED;
   p.JT = (int)jt;
   p.smem1 = (size_t)p.nmu * p.JT * p.pitch * p.elem + p.S * (p.elem + sizeof(int));
+  plan_stage1_staged(p);
+  int idx = pick_fast2(p);
+  if (idx >= 0) {
+    p.f2_variant = idx;
+    p.M1 = kS2Choices[idx].M1;
+    p.M2 = kS2Choices[idx].M2;
+    p.C1 = p.C2 = 2;
+    p.fast2 = 2;                 // chosen; set up when the device plan is built
+    make_fft_plan(p.M1, p.plan1);
+    make_fft_plan(p.M2, p.plan2);
+    return SOI_OK;
+  }
   return choose_split(p);
 }
 
@@ -401,6 +709,11 @@ int init_plan(soi_desc_t *d, size_t k)
   if (ce != cudaSuccess) { delete p; return SOI_ERR_CUDA; }
   rc = p->prec == SOI_PRECISION_FP64 ? build_tables<double>(*p) : build_tables<float>(*p);
   if (rc) { free_plan(p); return rc; }
+  if ((rc = upload_regtw())) { free_plan(p); return rc; }
+  if (p->fast2 == 2) {
+    p->fast2 = 0;
+    if ((rc = setup_fast2(*p, p->f2_variant))) { free_plan(p); return rc; }
+  }
   if (cudaMalloc(&p->d_T, p->S * p->Mh * p->elem) != cudaSuccess) { free_plan(p); return SOI_ERR_CUDA; }
   if (d->stream) {
     p->stream = (cudaStream_t)d->stream;
@@ -447,6 +760,7 @@ int compute_impl(soi_desc_t *d, const void *in, void *out, bool stage1_only)
   if (p->timing) CK(cudaEventRecord(p->ev[3], st));
   if (!d->device_ptr) CK(cudaMemcpyAsync(out, p->d_io, bytes, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
+  if ((rc = check_fast2(*p, st))) return rc;
   if (p->timing) {
     cudaEventElapsedTime(&p->ms[0], p->ev[0], p->ev[1]);
     cudaEventElapsedTime(&p->ms[2], p->ev[1], p->ev[2]);
@@ -627,7 +941,9 @@ int soi_segment_fft_demod_device(soi_desc_t *d, void *T_dev, void *out_dev)
   Plan *p = plan_of(d);
   if (!p) return SOI_ERR_NOT_INITIALISED;
   if (cudaSetDevice(p->device) != cudaSuccess) return SOI_ERR_CUDA;
-  return run_stage2(*p, T_dev, out_dev, p->stream);
+  int rc = run_stage2(*p, T_dev, out_dev, p->stream);
+  if (rc == SOI_OK && p->fast2) rc = check_fast2(*p, p->stream);
+  return rc;
 }
 
 int soi_plan_geometry(const soi_desc_t *d, cfft_size_t k, long long *info)
@@ -636,9 +952,10 @@ int soi_plan_geometry(const soi_desc_t *d, cfft_size_t k, long long *info)
   Plan p;
   int rc = plan_geometry(d, k, p);
   if (rc) return rc;
-  long long v[16] = { (long long)p.S, (long long)p.M, (long long)p.Mh, p.JT, p.atap, p.JR,
-                      (long long)p.smem1, p.M1, p.M2, p.C1, p.C2, (long long)p.smem_c,
-                      (long long)p.smem_r, p.planS.nst, p.plan1.nst, p.plan2.nst };
+  long long v[16] = { (long long)p.S, (long long)p.M, (long long)p.Mh, p.s1fast ? p.JT2 : p.JT, p.atap,
+                      p.s1fast ? p.JR2 : p.JR, (long long)(p.s1fast ? p.smem1b : p.smem1), p.M1, p.M2,
+                      p.C1, p.C2, (long long)p.smem_c, (long long)p.smem_r, p.planS.nst, p.plan1.nst,
+                      p.plan2.nst };
   memcpy(info, v, sizeof(v));
   return SOI_OK;
 }
@@ -669,6 +986,38 @@ int soi_window_tables(cfft_size_t N, cfft_size_t S, int n_mu, int d_mu, cfft_siz
   if (filt) for (size_t i = 0; i < f.size(); ++i) filt[i] = (double)f[i];
   if (phase) for (size_t i = 0; i < pr.size(); ++i) { phase[2 * i] = (double)pr[i]; phase[2 * i + 1] = (double)pi[i]; }
   if (W_inv) for (size_t i = 0; i < wr.size(); ++i) { W_inv[2 * i] = (double)wr[i]; W_inv[2 * i + 1] = (double)wi[i]; }
+  return SOI_OK;
+}
+
+int soi_mlp_param_count(void) { return kMlpParams; }
+
+int soi_mlp_forward_device(const float *params, const float *x, float *y, int n, void *stream)
+{
+  if (!params || !x || !y || n <= 0) return SOI_ERR_INVALID;
+  const int blocks = std::min(1024, (n + 127) / 128);
+  mlp_forward_kernel<<<blocks, 128, 0, (cudaStream_t)stream>>>(params, x, y, n);
+  CK(cudaGetLastError());
+  return SOI_OK;
+}
+
+int soi_mlp_grad_device(const float *params, const float *x, const float *y, int n, float *grad, float *loss,
+                        void *stream)
+{
+  if (!params || !x || !y || !grad || !loss || n <= 0) return SOI_ERR_INVALID;
+  cudaStream_t st = (cudaStream_t)stream;
+  CK(cudaMemsetAsync(grad, 0, kMlpParams * sizeof(float), st));
+  CK(cudaMemsetAsync(loss, 0, sizeof(float), st));
+  mlp_grad_kernel<<<(n + kMlpBlock - 1) / kMlpBlock, kMlpBlock, 0, st>>>(params, x, y, n, grad, loss);
+  CK(cudaGetLastError());
+  return SOI_OK;
+}
+
+int soi_mlp_adam_device(float *params, float *m, float *v, const float *grad, float lr, int step, void *stream)
+{
+  if (!params || !m || !v || !grad || step < 1) return SOI_ERR_INVALID;
+  mlp_adam_kernel<<<(kMlpParams + 255) / 256, 256, 0, (cudaStream_t)stream>>>(params, m, v, grad, kMlpParams, lr,
+                                                                               0.9f, 0.999f, 1e-8f, step);
+  CK(cudaGetLastError());
   return SOI_OK;
 }
 

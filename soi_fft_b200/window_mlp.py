@@ -1,0 +1,269 @@
+"""Learned window proposals for the SOI transform (no counterpart in the
+reference, whose windows are the analytic family of pfft.c:42-82 with the
+Pareto points of pfft.c:111-137).
+
+A small MLP (4 -> 64 -> 64 -> 1, GELU; CUDA forward/backward/Adam kernels in
+csrc/mlp_kernels.cuh) predicts log10 of the transform's relative L2 error
+from a window description (oversampling mu = n_mu/d_mu, taps B, tau, sigma).
+It is trained on errors that the method itself measures: the FP64 SOI
+transform of i.i.d. Gaussian inputs against an FP64 direct FFT.  Given a
+target accuracy, `propose` scans the network over (B, tau, sigma), takes the
+smallest B whose best predicted error beats the target with a margin, and
+`verify` runs the actual transform on a fresh input: the proposal is accepted
+only if the measured error meets the target.  Otherwise the analytic window
+(the reference's default, or its Pareto table) is used.
+
+Training and evaluation run on the GPU; torch provides device memory and the
+FP64 direct FFT used as the judge.
+"""
+import ctypes
+import math
+import os
+
+import numpy as np
+
+from . import lib, SoiDescriptor, PRECISION_FP64
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+WEIGHTS = os.path.join(HERE, "data", "window_mlp.npz")
+
+# oversampling pairs the network covers, and the N each is measured at
+# (M' = n_mu*M/d_mu must be integral: for 8/7 the length carries a factor 7)
+MU_PAIRS = [(5, 4), (8, 7), (9, 8)]
+NPARAMS = None
+
+# The reference's Pareto table, pfft.c:111-137: (mu, tau, sigma, B, SNR dB)
+PARETO = [
+    (1.25, 872 / 1024, 313.1715, 76, 289.2718), (1.25, 928 / 1024, 373.7314, 72, 288.1844),
+    (1.25, 818 / 1024, 267.4513, 64, 284.7614), (1.25, 0.899, 352.7647081, 60, 282),
+    (1.25, 764 / 1024, 213.2893, 60, 275.246), (1.25, 709 / 1024, 201.8235, 56, 266.6957),
+    (1.25, 0.782, 245.8927353, 54, 259), (1.25, 652 / 1024, 176.9743, 54, 258.2814),
+    (1.25, 591 / 1024, 154.7071, 50, 247.7459), (1.25, 512 / 1024, 121.0936, 44, 241.8972),
+    (1.25, 0.664, 182.5254421, 46, 239), (1.25, 0.578, 155.3322, 44, 233),
+    (1.25, 0.531, 136.5983707, 41, 220), (1.25, 383 / 1024, 104.1262, 42, 219.777),
+    (1.25, 0.4476, 119.2272, 38, 213), (1.25, 299 / 1024, 90.5391, 38, 210.1298),
+    (1.25, 0.373, 102.1115361, 36, 200), (1.25, 0.2927, 90.7306, 32, 193),
+    (1.25, 0.154, 73.2102363, 30, 179),
+    (1.125, 0.7238, 476.8683, 76, 213), (1.125, 0.6476, 363.891, 66, 193),
+    (1.5, 931 / 1024, 109.0712, 36, 289.6294), (1.5, 832 / 1024, 93.4329, 38, 289.4688),
+    (1.5, 0.0554, 36.6513, 22, 235),
+]
+
+TAU_RANGE = (0.08, 0.97)
+SIGMA_RANGE = (25.0, 800.0)
+B_RANGE = (12, 84)
+
+
+def nparams():
+    global NPARAMS
+    if NPARAMS is None:
+        NPARAMS = lib().soi_mlp_param_count()
+    return NPARAMS
+
+
+def features(n_mu, d_mu, B, tau, sigma):
+    """Normalised network inputs (arrays broadcast)."""
+    mu = np.asarray(n_mu, np.float64) / np.asarray(d_mu, np.float64)
+    return np.stack(np.broadcast_arrays((mu - 1.17) / 0.06, (np.asarray(B, np.float64) - 48.0) / 20.0,
+                                        (np.asarray(tau, np.float64) - 0.55) / 0.25,
+                                        (np.log(np.asarray(sigma, np.float64)) - 5.3) / 0.7), axis=-1)
+
+
+def length_for(n_mu, d_mu, log2n):
+    """A transform length near 2^log2n for which n_mu*M/d_mu is integral."""
+    return (1 << log2n) if d_mu in (1, 2, 4, 8, 16) else d_mu * (1 << (log2n - 3))
+
+
+# ------------------------------------------------------------ measurement --
+
+def measure_error(x, S, n_mu, d_mu, B, tau, sigma, X=None):
+    """rel-L2 of the FP64 SOI transform of the CUDA complex128 tensor x against
+    the FP64 direct FFT X (computed when not given)."""
+    import torch
+    if X is None:
+        X = torch.fft.fft(x)
+    d = SoiDescriptor(N=x.numel(), n_mu=n_mu, d_mu=d_mu, B=B, tau=float(tau), sigma=float(sigma),
+                      precision=PRECISION_FP64, device=x.device.index or 0)
+    try:
+        d.init(S)
+        y = torch.empty_like(x)
+        d.compute_into(x, y)
+    finally:
+        d.free()
+    e = float(torch.linalg.norm(y - X) / torch.linalg.norm(X))
+    if not math.isfinite(e):
+        e = 1.0
+    return e
+
+
+def sample_windows(rng, n, n_mu, d_mu):
+    B = rng.integers(max(B_RANGE[0], d_mu + 1), B_RANGE[1] + 1, size=n)
+    tau = rng.uniform(*TAU_RANGE, size=n)
+    sigma = np.exp(rng.uniform(np.log(SIGMA_RANGE[0]), np.log(SIGMA_RANGE[1]), size=n))
+    return B, tau, sigma
+
+
+def make_dataset(per_mu=1200, log2n=20, S=16, seed=0, device="cuda"):
+    """Measured (features, log10 error) pairs over the three oversampling pairs."""
+    import torch
+    rng = np.random.default_rng(seed)
+    feats, ys, raw = [], [], []
+    for (n, d) in MU_PAIRS:
+        N = length_for(n, d, log2n)
+        g = torch.Generator(device=device).manual_seed(seed + n)
+        x = torch.complex(torch.randn(N, generator=g, device=device, dtype=torch.float64),
+                          torch.randn(N, generator=g, device=device, dtype=torch.float64))
+        X = torch.fft.fft(x)
+        B, tau, sigma = sample_windows(rng, per_mu, n, d)
+        for b, t, s in zip(B, tau, sigma):
+            e = measure_error(x, S, n, d, int(b), t, s, X)
+            raw.append((n, d, int(b), t, s, e))
+            feats.append(features(n, d, b, t, s))
+            ys.append(max(np.log10(max(e, 1e-300)), -16.5))
+    return np.array(feats, np.float32), np.array(ys, np.float32), raw
+
+
+# ---------------------------------------------------------------- network --
+
+class WindowMLP:
+    """Parameters and Adam state in device memory; kernels from the C ABI."""
+
+    def __init__(self, params=None, seed=0, device="cuda"):
+        import torch
+        self.device = device
+        n = nparams()
+        if params is None:
+            rng = np.random.default_rng(seed)
+            p = np.zeros(n, np.float32)
+            # W1 64x4, W2 64x64, W3 64 (Glorot-style scale); biases zero
+            p[0:256] = rng.normal(0, np.sqrt(2.0 / 68), 256)
+            p[320:320 + 4096] = rng.normal(0, np.sqrt(2.0 / 128), 4096)
+            p[320 + 4096 + 64:320 + 4096 + 128] = rng.normal(0, np.sqrt(2.0 / 65), 64)
+            params = p
+        self.p = torch.tensor(np.asarray(params, np.float32), device=device)
+        self.m = torch.zeros_like(self.p)
+        self.v = torch.zeros_like(self.p)
+        self.g = torch.zeros_like(self.p)
+        self.loss = torch.zeros(1, dtype=torch.float32, device=device)
+        self.step = 0
+
+    @staticmethod
+    def _ptr(t):
+        return ctypes.c_void_p(t.data_ptr())
+
+    def forward(self, x):
+        import torch
+        x = torch.as_tensor(np.asarray(x, np.float32), device=self.device).contiguous()
+        y = torch.empty(x.shape[0], dtype=torch.float32, device=self.device)
+        rc = lib().soi_mlp_forward_device(self._ptr(self.p), self._ptr(x), self._ptr(y), x.shape[0], None)
+        if rc:
+            raise RuntimeError("soi_mlp_forward_device: %d" % rc)
+        return y
+
+    def grad(self, x, y):
+        """(loss, gradient) of mean squared error on device tensors x [n,4], y [n]."""
+        rc = lib().soi_mlp_grad_device(self._ptr(self.p), self._ptr(x), self._ptr(y), x.shape[0],
+                                       self._ptr(self.g), self._ptr(self.loss), None)
+        if rc:
+            raise RuntimeError("soi_mlp_grad_device: %d" % rc)
+        return self.loss, self.g
+
+    def train(self, x, y, steps=3000, lr=3e-3, lr_end=2e-4, batch=1024, seed=0):
+        import torch
+        xd = torch.as_tensor(np.asarray(x, np.float32), device=self.device).contiguous()
+        yd = torch.as_tensor(np.asarray(y, np.float32), device=self.device).contiguous()
+        n = xd.shape[0]
+        gen = torch.Generator(device="cpu").manual_seed(seed)
+        hist = []
+        for i in range(steps):
+            idx = torch.randint(0, n, (min(batch, n),), generator=gen).to(self.device)
+            xb, yb = xd[idx].contiguous(), yd[idx].contiguous()
+            self.grad(xb, yb)
+            self.step += 1
+            a = lr * (lr_end / lr) ** (i / max(1, steps - 1))
+            rc = lib().soi_mlp_adam_device(self._ptr(self.p), self._ptr(self.m), self._ptr(self.v),
+                                           self._ptr(self.g), ctypes.c_float(a), self.step, None)
+            if rc:
+                raise RuntimeError("soi_mlp_adam_device: %d" % rc)
+            if i % 200 == 0 or i == steps - 1:
+                hist.append(float(self.loss.item()))
+        return hist
+
+    def params_numpy(self):
+        return self.p.cpu().numpy()
+
+    def save(self, path=WEIGHTS, **meta):
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        np.savez(path, params=self.params_numpy(), **meta)
+
+    @classmethod
+    def load(cls, path=WEIGHTS, device="cuda"):
+        z = np.load(path)
+        return cls(params=z["params"], device=device)
+
+    # ---------------------------------------------------------- proposals --
+
+    def predict_best(self, n_mu, d_mu, ntau=48, nsig=48):
+        """For every B, the (tau, sigma) with the lowest predicted error."""
+        Bs = np.arange(max(B_RANGE[0], d_mu + 1), B_RANGE[1] + 1)
+        taus = np.linspace(*TAU_RANGE, ntau)
+        sigs = np.exp(np.linspace(np.log(SIGMA_RANGE[0]), np.log(SIGMA_RANGE[1]), nsig))
+        BB, TT, SS = np.meshgrid(Bs, taus, sigs, indexing="ij")
+        f = features(n_mu, d_mu, BB.ravel(), TT.ravel(), SS.ravel())
+        pred = self.forward(f).cpu().numpy().reshape(BB.shape)
+        k = pred.reshape(len(Bs), -1).argmin(1)
+        out = []
+        for i, b in enumerate(Bs):
+            it, isg = np.unravel_index(k[i], (ntau, nsig))
+            out.append((int(b), float(taus[it]), float(sigs[isg]), float(pred[i, it, isg])))
+        return out
+
+    def propose(self, n_mu, d_mu, target, margin=0.5):
+        """Candidates (B, tau, sigma, predicted log10 error) in increasing B
+        whose prediction beats log10(target) by `margin` decades."""
+        lt = math.log10(target)
+        return [c for c in self.predict_best(n_mu, d_mu) if c[3] <= lt - margin]
+
+
+def analytic_window(n_mu, d_mu, target, measure):
+    """The method without the network: the smallest-B Pareto point of the
+    reference's table for this mu whose measured error meets the target, else
+    the default window (pfft.c:87-91).  `measure(B, tau, sigma)` returns the
+    error."""
+    mu = n_mu / d_mu
+    for (m, tau, sigma, B, snr) in sorted((p for p in PARETO if abs(p[0] - mu) < 1e-9), key=lambda p: p[3]):
+        e = measure(B, tau, sigma)
+        if e <= target:
+            return B, tau, sigma, e
+    e = measure(72, 928 / 1024., 373.7314)
+    return 72, 928 / 1024., 373.7314, e
+
+
+def learned_window(net, n_mu, d_mu, target, measure, tries=4):
+    """A verified proposal: the first candidate (smallest B) whose measured
+    error meets the target; None when none of the first `tries` does."""
+    for (B, tau, sigma, pred) in net.propose(n_mu, d_mu, target)[:tries]:
+        e = measure(B, tau, sigma)
+        if e <= target:
+            return B, tau, sigma, e, pred
+    return None
+
+
+def main():
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="train the learned-window surrogate on the GPU")
+    ap.add_argument("--per-mu", type=int, default=1200)
+    ap.add_argument("--log2n", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--out", default=WEIGHTS)
+    a = ap.parse_args()
+    x, y, raw = make_dataset(per_mu=a.per_mu, log2n=a.log2n)
+    net = WindowMLP(seed=1)
+    hist = net.train(x, y, steps=a.steps)
+    net.save(a.out, dataset_x=x, dataset_y=y, loss_history=np.array(hist))
+    print(json.dumps({"samples": int(len(y)), "loss_first": hist[0], "loss_last": hist[-1]}))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,82 @@
+"""The learned-window surrogate: its CUDA forward/backward kernels against the
+CPU reference (oracle/mlp_ref.py), training, and what the trained network
+gains over the analytic window."""
+import ctypes
+import math
+import os
+
+import numpy as np
+import pytest
+
+import soi_fft_b200 as sb
+from oracle import mlp_ref
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+from soi_fft_b200 import window_mlp as wm  # noqa: E402
+
+
+def ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def rand_problem(n, seed):
+    rng = np.random.default_rng(seed)
+    p = rng.normal(0, 0.3, mlp_ref.NPARAMS).astype(np.float32)
+    x = rng.normal(0, 1, (n, 4)).astype(np.float32)
+    y = rng.normal(0, 1, n).astype(np.float32)
+    return p, x, y
+
+
+@pytest.mark.parametrize("n", [1, 31, 32, 200, 1000])
+def test_mlp_gradient_matches_cpu_reference(n):
+    p, x, y = rand_problem(n, n)
+    net = wm.WindowMLP(params=p)
+    xd, yd = torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda()
+    loss, g = net.grad(xd, yd)
+    ref_loss, ref_g = mlp_ref.loss_and_grad(p, x, y)
+    assert abs(loss.item() - ref_loss) <= 1e-5 * max(1.0, ref_loss)
+    gd = g.cpu().numpy().astype(np.float64)
+    assert np.linalg.norm(gd - ref_g) <= 1e-4 * np.linalg.norm(ref_g)
+
+
+def test_mlp_forward_matches_cpu_reference():
+    p, x, _ = rand_problem(5000, 3)
+    net = wm.WindowMLP(params=p)
+    y = net.forward(x).cpu().numpy()
+    ref = mlp_ref.forward(p, x)
+    assert np.max(np.abs(y - ref)) <= 1e-4 * max(1.0, np.max(np.abs(ref)))
+
+
+def test_mlp_training_fits_a_smooth_function():
+    rng = np.random.default_rng(4)
+    x = rng.uniform(-1.5, 1.5, (4096, 4)).astype(np.float32)
+    y = (np.sin(x[:, 0]) * x[:, 1] - 0.5 * x[:, 2] ** 2 + np.tanh(x[:, 3])).astype(np.float32)
+    net = wm.WindowMLP(seed=2)
+    hist = net.train(x, y, steps=1500, lr=3e-3, lr_end=3e-4, batch=512)
+    assert hist[-1] < 0.05 * hist[0]
+    pred = net.forward(x).cpu().numpy()
+    assert np.sqrt(np.mean((pred - y) ** 2)) < 0.1
+
+
+@pytest.mark.skipif(not os.path.exists(wm.WEIGHTS), reason="no trained weights (python -m soi_fft_b200.window_mlp)")
+@pytest.mark.parametrize("n_mu,d_mu,target", [(5, 4, 1e-11), (9, 8, 1e-9), (8, 7, 1e-8)])
+def test_learned_window_needs_fewer_taps_at_equal_accuracy(n_mu, d_mu, target):
+    # held-out evaluation at a larger length than training (N ~ 2^22, S = 32)
+    N = wm.length_for(n_mu, d_mu, 22)
+    S = 32
+    g = torch.Generator(device="cuda").manual_seed(1234)
+    x = torch.complex(torch.randn(N, generator=g, device="cuda", dtype=torch.float64),
+                      torch.randn(N, generator=g, device="cuda", dtype=torch.float64))
+    X = torch.fft.fft(x)
+    measure = lambda B, tau, sigma: wm.measure_error(x, S, n_mu, d_mu, int(B), tau, sigma, X)
+    net = wm.WindowMLP.load()
+    learned = wm.learned_window(net, n_mu, d_mu, target, measure)
+    base = wm.analytic_window(n_mu, d_mu, target, measure)
+    assert learned is not None, "no proposal met the target"
+    B, tau, sigma, err, pred = learned
+    assert err <= target                      # the oracle is the judge
+    if base[3] <= target:
+        assert B <= base[0]
+    print("mu=%d/%d target=%.0e learned B=%d (err %.2e, pred %.2e) analytic B=%d (err %.2e)"
+          % (n_mu, d_mu, target, B, err, 10 ** pred, base[0], base[3]))

@@ -209,3 +209,39 @@ def test_out_of_place_leaves_input_and_matches_in_place(prec):
     d.free()
     assert np.array_equal(out.cpu().numpy(), inplace)
     assert np.array_equal(host_out, inplace)
+
+
+@pytest.mark.parametrize("prec,tol", [(sb.PRECISION_FP64, 1e-13), (sb.PRECISION_SPLIT_FP32, 2e-6)])
+@pytest.mark.parametrize("N,S", [(1 << 20, 8), (1 << 22, 128), (1 << 18, 64)])
+def test_fast_paths_agree_with_fallback_kernels(prec, tol, N, S, monkeypatch):
+    dt = np.complex128 if prec == sb.PRECISION_FP64 else np.complex64
+    x = on_gpu(signals.gaussian(N, 21, dt))
+    outs = []
+    for fast in ("1", "0"):
+        monkeypatch.setenv("SOI_STAGE1_FAST", fast)
+        monkeypatch.setenv("SOI_STAGE2_FAST", fast)
+        d = sb.SoiDescriptor(N=N, precision=prec).init(S)
+        outs.append(d.compute(x.clone()).cpu().numpy().astype(np.complex128))
+        d.free()
+    assert rel_l2(outs[0], outs[1]) <= tol
+
+
+def test_fp64_first_plan_in_a_fresh_process():
+    # every plan must set up all device tables it uses: an FP64 plan made
+    # first in a process (no split-form plan before it) must be exact
+    import subprocess
+    import sys
+    import os
+    code = ("import numpy as np, soi_fft_b200 as sb\n"
+            "from oracle import oracle\n"
+            "from tests import signals\n"
+            "for N, S in ((1 << 16, 8), (1 << 18, 32), (1 << 18, 64)):\n"
+            "    x = signals.gaussian(N, 5)\n"
+            "    y = sb.soi_fft(x, S)\n"
+            "    r = oracle.compute_soi(x, S)\n"
+            "    e = np.linalg.norm(y - r) / np.linalg.norm(r)\n"
+            "    assert e < 1e-12, (N, S, e)\n"
+            "print('ok')\n")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "ok" in r.stdout, r.stderr[-2000:]

@@ -136,3 +136,65 @@ __device__ __forceinline__ void tile_fft_smem(V *sm, int C, int PP, int PC, cons
 }
 
 }  // namespace soi
+
+namespace soi {
+
+// tile_fft_smem with the tile geometry known at compile time: C columns,
+// shared index (pos + pos/RL)*PP + col*PC, NT threads.  Column and position
+// come from shifts and constant multiplies instead of runtime divisions.
+template <typename V, int R0, int R1, int R2, int C, int PP, int PC, int NT, class Emit>
+__device__ __forceinline__ void tile_fft_ct(V *sm, const V *__restrict__ tw, const Emit &emit)
+{
+  constexpr int RL = (R2 > 1) ? R2 : R1;
+  constexpr int L = R0 * R1 * R2;
+  constexpr int span0 = L / R0;
+  auto sidx = [](int col, int pos) { return (pos + pos / RL) * PP + col * PC; };
+  {
+    constexpr int n = C * span0;
+#pragma unroll 1
+    for (int q = threadIdx.x; q < n; q += NT) {
+      const int col = q % C, i = q / C;
+      V v[R0];
+#pragma unroll
+      for (int r = 0; r < R0; ++r) v[r] = sm[sidx(col, i + r * span0)];
+      RegDFT<V, R0>::run(v);
+#pragma unroll
+      for (int k = 0; k < R0; ++k) sm[sidx(col, i + k * span0)] = (k && i) ? cmul(v[k], tw[i * k]) : v[k];
+    }
+  }
+  __syncthreads();
+  if constexpr (R2 > 1) {
+    constexpr int span1 = span0 / R1;
+    constexpr int n = C * (L / R1);
+#pragma unroll 1
+    for (int q = threadIdx.x; q < n; q += NT) {
+      const int col = q % C, t = q / C;
+      const int blk = t / span1, i = t - blk * span1;
+      const int base = blk * span0 + i;
+      V v[R1];
+#pragma unroll
+      for (int r = 0; r < R1; ++r) v[r] = sm[sidx(col, base + r * span1)];
+      RegDFT<V, R1>::run(v);
+#pragma unroll
+      for (int k = 0; k < R1; ++k) sm[sidx(col, base + k * span1)] = (k && i) ? cmul(v[k], tw[i * k * R0]) : v[k];
+    }
+    __syncthreads();
+  }
+  {
+    constexpr int n = C * (L / RL);
+#pragma unroll 1
+    for (int q = threadIdx.x; q < n; q += NT) {
+      const int col = q % C, blk = q / C;
+      V v[RL];
+#pragma unroll
+      for (int r = 0; r < RL; ++r) v[r] = sm[sidx(col, blk * RL + r)];
+      RegDFT<V, RL>::run(v);
+      int fbase;
+      if constexpr (R2 > 1) fbase = (blk / R1) + R0 * (blk % R1);
+      else fbase = blk;
+      emit.template run<RL>(col, fbase, L / RL, v);
+    }
+  }
+}
+
+}  // namespace soi

@@ -50,7 +50,8 @@ struct Plan {
   int *d_vlc_words = nullptr, *d_vlc_n = nullptr, *d_vlc_emax = nullptr;
   long vlc_stride = 0;
   // persistent stage 2 (split form): compiled radix split and its state
-  int fast2 = 0;               // 0: two-kernel stage 2, 1: persistent kernel
+  int fast2 = 0;               // 0: two-kernel stage 2, 1: runtime-geometry persistent kernel,
+                               // 3: compile-time-geometry persistent kernel (2, 4: chosen, not set up)
   int f2_variant = 0;
   int f2_grid = 0;
   size_t f2_smem = 0;
@@ -60,6 +61,8 @@ struct Plan {
   double2 *d_dlo = nullptr, *d_dhi = nullptr;
   int dlo_bits = 11;
   void (*f2_kernel)(S2Args) = nullptr;
+  void (*f2ct_kernel)(S2ArgsCT) = nullptr;   // compile-time-geometry stage 2 (fast2 == 3)
+  void *d_ph2 = nullptr;            // [M2] complex exp(-i pi kappa M1 k2 / M)
   unsigned int *d_sync = nullptr;   // [0] counter, [1] err, [2..2+S) done1
   // staged stage 1
   int s1fast = 0, JR2 = 0, JT2 = 0, AC = 0, buf_elems = 0;
@@ -290,7 +293,8 @@ const S2Choice kS2Choices[] = {
 // SOI_STAGE2_VARIANT=2 selects the two-stage (radix-64) one where compiled.
 int pick_fast2(const Plan &p)
 {
-  if (p.prec != SOI_PRECISION_SPLIT_FP32 || env_int("SOI_STAGE2_FAST", 1) == 0) return -1;
+  if (p.prec != SOI_PRECISION_SPLIT_FP32 || env_int("SOI_STAGE2_FAST", 1) == 0 ||
+      env_int("SOI_STAGE2_KERNEL", 3) != 2) return -1;
   const bool want2 = env_int("SOI_STAGE2_VARIANT", 0) == 2;
   int best = -1;
   for (int i = 0; i < (int)(sizeof(kS2Choices) / sizeof(kS2Choices[0])); ++i) {
@@ -322,6 +326,124 @@ int upload_regtw()
   return SOI_OK;
 }
 
+// ---- stage 2 with compile-time geometry ----------------------------------------
+
+using S2KernelCT = void (*)(S2ArgsCT);
+struct S2ChoiceCT { int M1, M2, elem, nt; size_t smem; S2KernelCT k; };
+
+#define SOI_S2CT(R, a0, a1, a2, b0, b1, b2)                                                   \
+  { a0 * a1 * a2, b0 * b1 * b2, (int)sizeof(typename cplx_of<R>::type), 256,                 \
+    (size_t)S2Geom<R, a0, a1, a2, b0, b1, b2, 256>::BUF * S2Geom<R, a0, a1, a2, b0, b1, b2, 256>::E, \
+    k_stage2_ct<R, a0, a1, a2, b0, b1, b2, 256> }
+
+const S2ChoiceCT kS2CT[] = {
+  SOI_S2CT(float, 10, 16, 16, 8, 16, 16),   // M' = 2560 x 2048 (N = 2^29, S = 128; 2^28, 64)
+  SOI_S2CT(float, 10, 16, 16, 4, 16, 16),   // 2560 x 1024
+  SOI_S2CT(float, 5, 16, 16, 4, 16, 16),    // 1280 x 1024
+  SOI_S2CT(float, 5, 16, 16, 8, 8, 8),      // 1280 x 512
+  SOI_S2CT(float, 10, 8, 8, 4, 16, 16),     // 640 x 1024
+  SOI_S2CT(float, 10, 8, 8, 8, 8, 8),       // 640 x 512
+  SOI_S2CT(float, 5, 8, 8, 8, 8, 8),        // 320 x 512
+  SOI_S2CT(float, 5, 8, 8, 4, 8, 8),        // 320 x 256
+  SOI_S2CT(double, 10, 16, 16, 8, 16, 16),
+  SOI_S2CT(double, 10, 16, 16, 4, 16, 16),
+  SOI_S2CT(double, 5, 16, 16, 4, 16, 16),
+  SOI_S2CT(double, 5, 16, 16, 8, 8, 8),
+  SOI_S2CT(double, 10, 8, 8, 4, 16, 16),
+  SOI_S2CT(double, 10, 8, 8, 8, 8, 8),
+  SOI_S2CT(double, 5, 8, 8, 8, 8, 8),
+  SOI_S2CT(double, 5, 8, 8, 4, 8, 8),
+};
+#undef SOI_S2CT
+
+// index into kS2CT for M' and the element size, or -1
+int pick_s2ct(const Plan &p)
+{
+  // SOI_STAGE2_KERNEL: 3 this kernel (default), 2 the runtime-geometry
+  // persistent kernel, 1 the two-kernel path; SOI_STAGE2_FAST=0 also selects
+  // the two-kernel path
+  if (env_int("SOI_STAGE2_KERNEL", 3) != 3 || env_int("SOI_STAGE2_FAST", 1) == 0) return -1;
+  for (int i = 0; i < (int)(sizeof(kS2CT) / sizeof(kS2CT[0])); ++i)
+    if ((long long)kS2CT[i].M1 * kS2CT[i].M2 == (long long)p.Mh && kS2CT[i].elem == (int)p.elem) return i;
+  return -1;
+}
+
+// demodulation tables shared by both persistent kernels: amp[k] = 1/y_W(k/M - 1/2)
+// for k <= M/2 (even about M/2), exp(-i pi kappa k/M) two-level in FP64, and
+// (compile-time kernel) ph2[k2] = exp(-i pi kappa M1 k2/M)
+template <typename R>
+int build_demod_tables(Plan &p, bool with_ph2)
+{
+  const size_t M = p.M, half = M / 2 + 1;
+  const long double sq = sqrtl((long double)p.sigma);
+  std::vector<R> af(half);
+  for (size_t i = 0; i < half; ++i) {
+    long double t = (long double)i / (long double)M - 0.5L;
+    long double y = (erfcl(sq * (t - p.tau / 2.0L)) - erfcl(sq * (t + p.tau / 2.0L))) / (2.0L * p.tau);
+    af[i] = (R)(1.0L / y);
+  }
+  int rc;
+  if ((rc = upload(&p.d_amp, af.data(), af.size() * sizeof(R)))) return rc;
+  const long long kappa = (long long)p.B - p.dmu;
+  auto phase = [&](long long k, long double *o) {
+    long long q = (long long)(((unsigned long long)kappa * (unsigned long long)k) % (2ULL * M));
+    long double ang = -kPi * (long double)q / (long double)M;
+    o[0] = cosl(ang);
+    o[1] = sinl(ang);
+  };
+  const long long nlo = 1LL << p.dlo_bits, nhi = (long long)(M >> p.dlo_bits) + 2;
+  std::vector<double> lo(2 * nlo), hi(2 * nhi);
+  long double o[2];
+  for (long long e = 0; e < nlo; ++e) { phase(e, o); lo[2 * e] = (double)o[0]; lo[2 * e + 1] = (double)o[1]; }
+  for (long long h = 0; h < nhi; ++h) { phase(h * nlo, o); hi[2 * h] = (double)o[0]; hi[2 * h + 1] = (double)o[1]; }
+  if ((rc = upload((void **)&p.d_dlo, lo.data(), lo.size() * sizeof(double)))) return rc;
+  if ((rc = upload((void **)&p.d_dhi, hi.data(), hi.size() * sizeof(double)))) return rc;
+  if (with_ph2) {
+    std::vector<R> ph(2 * (size_t)p.M2);
+    for (int k2 = 0; k2 < p.M2; ++k2) {
+      phase((long long)p.M1 * k2, o);
+      ph[2 * k2] = (R)o[0];
+      ph[2 * k2 + 1] = (R)o[1];
+    }
+    if ((rc = upload(&p.d_ph2, ph.data(), ph.size() * sizeof(R)))) return rc;
+  }
+  return SOI_OK;
+}
+
+int setup_s2ct(Plan &p, int idx)
+{
+  const S2ChoiceCT &c = kS2CT[idx];
+  p.M1 = c.M1; p.M2 = c.M2;
+  p.C1 = p.C2 = 32 / c.elem;
+  p.f2_smem = c.smem;
+  p.f2ct_kernel = c.k;
+  CK(cudaFuncSetAttribute(c.k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.f2_smem));
+  int occ = 0, nsm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, c.k, c.nt, p.f2_smem));
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, p.device));
+  if (occ < 1) return SOI_ERR_UNSUPPORTED;
+  p.f2_grid = occ * nsm;
+  CK(cudaMalloc(&p.d_sync, (p.S + 2) * sizeof(unsigned int)));
+  int rc = p.prec == SOI_PRECISION_FP64 ? build_demod_tables<double>(p, true) : build_demod_tables<float>(p, true);
+  if (rc) return rc;
+  p.fast2 = 3;
+  return SOI_OK;
+}
+
+int launch_s2ct(Plan &p, void *T, void *out, cudaStream_t st)
+{
+  S2ArgsCT a;
+  a.T = T; a.out = out; a.tw1 = p.d_tw1; a.tw2 = p.d_tw2; a.xlo = p.d_xlo; a.xhi = p.d_xhi;
+  a.amp = p.d_amp; a.dlo = p.d_dlo; a.dhi = p.d_dhi; a.ph2 = p.d_ph2;
+  a.lo_bits = p.lo_bits; a.dlo_bits = p.dlo_bits; a.M = (int)p.M; a.S = (int)p.S;
+  a.discard = env_int("SOI_STAGE2_DISCARD", 1);
+  a.counter = p.d_sync; a.err = (int *)(p.d_sync + 1); a.done1 = p.d_sync + 2;
+  CK(cudaMemsetAsync(p.d_sync, 0, (p.S + 2) * sizeof(unsigned int), st));
+  p.f2ct_kernel<<<p.f2_grid, 256, p.f2_smem, st>>>(a);
+  CK(cudaGetLastError());
+  return SOI_OK;
+}
+
 int setup_fast2(Plan &p, int idx)
 {
   const S2Choice &c = kS2Choices[idx];
@@ -345,33 +467,10 @@ int setup_fast2(Plan &p, int idx)
   if (occ < 1) return SOI_ERR_UNSUPPORTED;
   p.f2_grid = occ * nsm;
   CK(cudaMalloc(&p.d_sync, (p.S + 2) * sizeof(unsigned int)));
-  // demodulation W_inv[k] = exp(-i pi kappa k/M) * amp[k] (pfft.c:68-82):
-  // amp = 1/y_W(k/M - 1/2) is even about M/2, kept for k <= M/2 and rounded
-  // once; the phase is formed in FP64 from two tables
+  // demodulation W_inv[k] = exp(-i pi kappa k/M) * amp[k] (pfft.c:68-82)
   {
-    const size_t M = p.M, half = M / 2 + 1;
-    const long double sq = sqrtl((long double)p.sigma);
-    std::vector<float> af(half);
-    for (size_t i = 0; i < half; ++i) {
-      long double t = (long double)i / (long double)M - 0.5L;
-      long double y = (erfcl(sq * (t - p.tau / 2.0L)) - erfcl(sq * (t + p.tau / 2.0L))) / (2.0L * p.tau);
-      af[i] = (float)(1.0L / y);
-    }
-    int rc;
-    if ((rc = upload(&p.d_amp, af.data(), af.size() * sizeof(float)))) return rc;
-    const long long kappa = (long long)p.B - p.dmu;
-    const long long nlo = 1LL << p.dlo_bits, nhi = (long long)(M >> p.dlo_bits) + 2;
-    std::vector<double> lo(2 * nlo), hi(2 * nhi);
-    auto phase = [&](long long k, double *o) {
-      long long q = (long long)(((unsigned long long)kappa * (unsigned long long)k) % (2ULL * M));
-      long double ang = -kPi * (long double)q / (long double)M;
-      o[0] = (double)cosl(ang);
-      o[1] = (double)sinl(ang);
-    };
-    for (long long e = 0; e < nlo; ++e) phase(e, &lo[2 * e]);
-    for (long long h = 0; h < nhi; ++h) phase(h * nlo, &hi[2 * h]);
-    if ((rc = upload((void **)&p.d_dlo, lo.data(), lo.size() * sizeof(double)))) return rc;
-    if ((rc = upload((void **)&p.d_dhi, hi.data(), hi.size() * sizeof(double)))) return rc;
+    int rc = build_demod_tables<float>(p, false);
+    if (rc) return rc;
   }
   p.fast2 = 1;
   return SOI_OK;
@@ -531,6 +630,7 @@ int run_stage1(Plan &p, const void *alpha, void *T, cudaStream_t st)
 
 int run_stage2(Plan &p, void *T, void *out, cudaStream_t st)
 {
+  if (p.fast2 == 3) return launch_s2ct(p, T, out, st);
   if (p.fast2) return launch_fast2(p, T, out, st);
   return p.prec == SOI_PRECISION_FP64 ? launch_seg_t<double>(p, T, out, st)
                                       : launch_seg_t<float>(p, T, out, st);
@@ -652,7 +752,7 @@ void free_plan(Plan *p)
   cudaSetDevice(p->device);
   void *bufs[] = { p->d_filt, p->d_phase, p->d_twS, p->d_tw1, p->d_tw2, p->d_winv, p->d_wsmall,
                    p->d_permS, p->d_perm1, p->d_perm2, p->d_xlo, p->d_xhi, p->d_T, p->d_io,
-                   p->d_vlc_x, p->d_vlc_words, p->d_vlc_n, p->d_vlc_emax, p->d_sync, p->d_filt2, p->d_amp, p->d_dlo, p->d_dhi };
+                   p->d_vlc_x, p->d_vlc_words, p->d_vlc_n, p->d_vlc_emax, p->d_sync, p->d_filt2, p->d_amp, p->d_dlo, p->d_dhi, p->d_ph2 };
   for (void *b : bufs) if (b) cudaFree(b);
   for (auto &e : p->ev) if (e) cudaEventDestroy(e);
   if (p->own_stream && p->stream) cudaStreamDestroy(p->stream);
@@ -686,6 +786,17 @@ int plan_geometry(const soi_desc_t *d, size_t k, Plan &p)
   p.JT = (int)jt;
   p.smem1 = (size_t)p.nmu * p.JT * p.pitch * p.elem + p.S * (p.elem + sizeof(int));
   plan_stage1_staged(p);
+  const int ict = pick_s2ct(p);
+  if (ict >= 0) {
+    p.f2_variant = ict;
+    p.M1 = kS2CT[ict].M1;
+    p.M2 = kS2CT[ict].M2;
+    p.C1 = p.C2 = 32 / kS2CT[ict].elem;
+    p.fast2 = 4;                 // chosen; set up when the device plan is built
+    make_fft_plan(p.M1, p.plan1);
+    make_fft_plan(p.M2, p.plan2);
+    return SOI_OK;
+  }
   int idx = pick_fast2(p);
   if (idx >= 0) {
     p.f2_variant = idx;
@@ -713,6 +824,9 @@ int init_plan(soi_desc_t *d, size_t k)
   if (p->fast2 == 2) {
     p->fast2 = 0;
     if ((rc = setup_fast2(*p, p->f2_variant))) { free_plan(p); return rc; }
+  } else if (p->fast2 == 4) {
+    p->fast2 = 0;
+    if ((rc = setup_s2ct(*p, p->f2_variant))) { free_plan(p); return rc; }
   }
   if (cudaMalloc(&p->d_T, p->S * p->Mh * p->elem) != cudaSuccess) { free_plan(p); return SOI_ERR_CUDA; }
   if (d->stream) {

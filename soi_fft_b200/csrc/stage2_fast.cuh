@@ -237,4 +237,212 @@ __global__ void __launch_bounds__(128, 4) k_stage2_persistent(S2Args a)
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Stage 2 with the tile geometry fixed at compile time.
+//
+// Tasks and schedule as in k_stage2_persistent.  Differences:
+//  * C1 = C2 = 32 bytes / element size: every strided row run of a tile
+//    (pass-1 loads and stores, pass-2 output stores) is one full 32-byte
+//    sector, so each L2 request moves a whole sector.
+//  * Epilogue factors come from per-task tables instead of scattered lookups.
+//    Pass 1: w_{M'}^(m2*f) for f = fbase + fstep*k is base(m2*fbase) times
+//    step[col][k] = w_{M'}^(m2*fstep*k), the C1 x RL step table built per
+//    task in shared memory.  Pass 2: W_inv[k], k = k1 + M1*k2, is
+//    amp[min(k, M-k)] * ph(k1) * ph(M1*k2) with ph(k) = exp(-i pi kappa k/M);
+//    ph(k1) per task in shared memory, ph(M1*k2) from an M2-entry table.
+//    Every table entry is FP64-generated and rounded once; the products are
+//    formed in the working precision.
+//  * The CTA claims its next task while it works on the current one.  A CTA
+//    holds at most one claimed task it has not started, and a pass-2 task only
+//    waits on tasks with smaller indices, so the lowest unfinished task can
+//    always run.
+// ---------------------------------------------------------------------------
+
+struct S2ArgsCT {
+  void *T;                    // [S][Mh] pass-1 input, intermediate in place
+  void *out;                  // [S][M]
+  const void *tw1, *tw2;      // exp(-2 pi i m/M1), exp(-2 pi i m/M2)
+  const double2 *xlo, *xhi;   // w_{M'}^e two-level, FP64
+  const void *amp;            // [M/2 + 1] real
+  const double2 *dlo, *dhi;   // exp(-i pi kappa k/M) two-level, FP64
+  const void *ph2;            // [M2] complex: exp(-i pi kappa M1 k2 / M)
+  int lo_bits, dlo_bits;
+  int M, S;
+  int discard;
+  unsigned int *counter, *done1;
+  int *err;
+};
+
+template <typename V>
+__device__ __forceinline__ V two_level(const double2 *lo, const double2 *hi, int bits, int e)
+{
+  const double2 l = __ldg(lo + (e & ((1 << bits) - 1)));
+  const double2 h = __ldg(hi + (e >> bits));
+  return cmk<V>((decltype(V::x))(h.x * l.x - h.y * l.y), (decltype(V::x))(h.x * l.y + h.y * l.x));
+}
+
+template <typename V, int C1, int M2, int RL> struct EmitColsCT {
+  V *Tseg; int m2_0; const V *step; const S2ArgsCT *a;
+  template <int RLx> __device__ __forceinline__ void run(int col, int fbase, int fstep, V *v) const
+  {
+    static_assert(RLx == RL, "last radix");
+    const int m2 = m2_0 + col;
+    const V base = two_level<V>(a->xlo, a->xhi, a->lo_bits, m2 * fbase);
+    V *dst = Tseg + fbase * M2 + m2;
+    dst[0] = cmul(v[0], base);
+#pragma unroll
+    for (int k = 1; k < RL; ++k) dst[k * fstep * M2] = cmul(v[k], cmul(base, step[col * RL + k]));
+  }
+};
+
+template <typename V, int M1, int RL> struct EmitRowsCT {
+  V *oseg; int k1_0; const V *ph1; const S2ArgsCT *a;
+  template <int RLx> __device__ __forceinline__ void run(int col, int fbase, int fstep, V *v) const
+  {
+    static_assert(RLx == RL, "last radix");
+    using Rr = decltype(V::x);
+    const int k1 = k1_0 + col;
+    const int M = a->M;
+    const V p1 = ph1[col];
+    const V *ph2 = reinterpret_cast<const V *>(a->ph2);
+    const Rr *amp = reinterpret_cast<const Rr *>(a->amp);
+#pragma unroll
+    for (int j = 0; j < RL; ++j) {
+      const int k2 = fbase + fstep * j;
+      const int k = k1 + M1 * k2;
+      if (k < M) {
+        const int km = k <= M - k ? k : M - k;
+        const V w = cscale(cmul(p1, __ldg(ph2 + k2)), __ldg(amp + km));
+        stcs(oseg + k, cmul(v[j], w));
+      }
+    }
+  }
+};
+
+template <int base, int mod, int rem> constexpr int round_up_to_residue()
+{
+  int x = base;
+  while (x % mod != rem) ++x;
+  return x;
+}
+
+template <typename R, int A0, int A1, int A2, int B0, int B1, int B2, int NT>
+struct S2Geom {
+  using V = typename cplx_of<R>::type;
+  static constexpr int E = (int)sizeof(V);
+  static constexpr int C = 32 / E;                          // columns (rows) per task
+  static constexpr int M1 = A0 * A1 * A2, M2 = B0 * B1 * B2;
+  static constexpr int RLA = A2 > 1 ? A2 : A1, RLB = B2 > 1 ? B2 : B1;
+  static constexpr int NT1 = M2 / C, NT2 = M1 / C, PER = NT1 + NT2;
+  // pass-2 row pitch: the C rows land on disjoint banks in the last stage
+  // (8-byte elements: pitch = 4 mod 16; 16-byte elements: pitch = 4 mod 8)
+  static constexpr int PS2 = E == 8 ? round_up_to_residue<M2 + M2 / RLB, 16, 4>()
+                                    : round_up_to_residue<M2 + M2 / RLB, 8, 4>();
+  static constexpr int BUF1 = (M1 + M1 / RLA) * C, BUF2 = PS2 * C;
+  static constexpr int BUF = BUF1 > BUF2 ? BUF1 : BUF2;
+  static constexpr int TAB = C * RLA;                       // shared table entries
+};
+
+template <typename R, int A0, int A1, int A2, int B0, int B1, int B2, int NT>
+__global__ void __launch_bounds__(NT, 2) k_stage2_ct(S2ArgsCT a)
+{
+  using G = S2Geom<R, A0, A1, A2, B0, B1, B2, NT>;
+  using V = typename G::V;
+  constexpr int C = G::C, M1 = G::M1, M2 = G::M2, RLA = G::RLA, RLB = G::RLB;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V *buf = reinterpret_cast<V *>(smem_raw);
+  __shared__ V s_tab[G::TAB];
+  __shared__ unsigned int s_task;
+  __shared__ int s_ok;
+  const int tid = threadIdx.x;
+  const unsigned int total = (unsigned int)a.S * G::PER;
+  unsigned int next = 0;
+  if (tid == 0) next = atomicAdd(a.counter, 1u);
+
+  for (;;) {
+    if (tid == 0) {
+      unsigned int t = next;
+      if (t < total) next = atomicAdd(a.counter, 1u);       // claim the following task now
+      if (*(volatile int *)a.err) t = total;
+      int ok = 1;
+      if (t < total && t >= (unsigned int)G::NT1) {
+        const unsigned int u = t - G::NT1;
+        const int blk = (int)(u / G::PER), r = (int)(u % G::PER);
+        if (blk >= a.S - 1 || r >= G::NT1) {                // pass-2 task of segment blk
+          long long it = 0;
+          while (ld_acquire_u32(a.done1 + blk) < (unsigned int)G::NT1) {
+            if (++it > kWaitLimit) { atomicExch(a.err, 1); ok = 0; break; }
+            __nanosleep(128);
+          }
+        }
+      }
+      s_task = t;
+      s_ok = ok;
+    }
+    __syncthreads();
+    const unsigned int t = s_task;
+    if (t >= total || !s_ok) break;
+    int kind, seg, tile;
+    if (t < (unsigned int)G::NT1) { kind = 1; seg = 0; tile = (int)t; }
+    else {
+      const unsigned int u = t - G::NT1;
+      const int blk = (int)(u / G::PER), r = (int)(u % G::PER);
+      if (blk < a.S - 1 && r < G::NT1) { kind = 1; seg = blk + 1; tile = r; }
+      else { kind = 2; seg = blk; tile = r - (blk < a.S - 1 ? G::NT1 : 0); }
+    }
+    V *Tseg = reinterpret_cast<V *>(a.T) + (size_t)seg * ((size_t)M1 * M2);
+    if (kind == 1) {
+      const int m2_0 = tile * C;
+      // rows m1 of C columns: 32 bytes = 2 chunks of 16
+      constexpr int EPC = 16 / G::E;                        // elements per 16-byte chunk
+      for (int q = tid; q < M1 * 2; q += NT) {
+        const int row = q >> 1, h = q & 1;
+        cp_async_16cg(buf + (row + row / RLA) * C + h * EPC, Tseg + row * M2 + m2_0 + h * EPC);
+      }
+      cp_commit();
+      if (tid < C * RLA) {
+        const int col = tid / RLA, k = tid % RLA;
+        s_tab[tid] = two_level<V>(a.xlo, a.xhi, a.lo_bits, (m2_0 + col) * ((M1 / RLA) * k));
+      }
+      cp_wait_all();
+      __syncthreads();
+      EmitColsCT<V, C, M2, RLA> e{ Tseg, m2_0, s_tab, &a };
+      tile_fft_ct<V, A0, A1, A2, C, C, 1, NT>(buf, reinterpret_cast<const V *>(a.tw1), e);
+      __syncthreads();
+      if (tid == 0) {
+        __threadfence();
+        atomicAdd(a.done1 + seg, 1u);
+      }
+    } else {
+      const int k1_0 = tile * C;
+      const V *src = Tseg + k1_0 * M2;
+      if constexpr (G::E == 16) {
+        for (int q = tid; q < C * M2; q += NT) {
+          const int col = q / M2, pos = q % M2;
+          cp_async_16cg(buf + (pos + pos / RLB) + col * G::PS2, src + q);
+        }
+      } else {
+        for (int q = tid; q < C * M2; q += NT) {
+          const int col = q / M2, pos = q % M2;
+          cp_async_8(buf + (pos + pos / RLB) + col * G::PS2, src + q);
+        }
+      }
+      cp_commit();
+      if (tid < C) s_tab[tid] = two_level<V>(a.dlo, a.dhi, a.dlo_bits, k1_0 + tid);
+      cp_wait_all();
+      __syncthreads();
+      if (a.discard) {
+        // the tile's rows are in shared memory now; their L2 lines are dead
+        const char *base = reinterpret_cast<const char *>(src);
+        constexpr int nlines = C * M2 * G::E / 128;
+        for (int l = tid; l < nlines; l += NT) discard_l2_line(base + l * 128);
+      }
+      EmitRowsCT<V, M1, RLB> e{ reinterpret_cast<V *>(a.out) + (size_t)seg * a.M, k1_0, s_tab, &a };
+      tile_fft_ct<V, B0, B1, B2, C, 1, G::PS2, NT>(buf, reinterpret_cast<const V *>(a.tw2), e);
+    }
+    __syncthreads();
+  }
+}
+
 }  // namespace soi

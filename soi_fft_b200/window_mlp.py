@@ -50,6 +50,16 @@ PARETO = [
 ]
 
 TAU_RANGE = (0.08, 0.97)
+# training targets are log10(error) clipped to [-16.5, 1]: every window whose
+# error is above 10 is equally useless, and the clip keeps the blown-up ones
+# (errors up to 1e15 where the window's frequency response nearly vanishes)
+# from taking the network's capacity
+Y_CLIP = (-16.5, 1.0)
+
+
+def clip_target(y):
+    return np.clip(y, *Y_CLIP)
+
 SIGMA_RANGE = (25.0, 800.0)
 B_RANGE = (12, 84)
 
@@ -119,7 +129,7 @@ def make_dataset(per_mu=1200, log2n=20, S=16, seed=0, device="cuda"):
             e = measure_error(x, S, n, d, int(b), t, s, X)
             raw.append((n, d, int(b), t, s, e))
             feats.append(features(n, d, b, t, s))
-            ys.append(max(np.log10(max(e, 1e-300)), -16.5))
+            ys.append(clip_target(np.log10(max(e, 1e-300))))
     return np.array(feats, np.float32), np.array(ys, np.float32), raw
 
 
@@ -257,8 +267,15 @@ def main():
     ap.add_argument("--log2n", type=int, default=20)
     ap.add_argument("--steps", type=int, default=4000)
     ap.add_argument("--out", default=WEIGHTS)
+    ap.add_argument("--from-dataset", default=None,
+                    help="retrain on the measurements stored in a weights file instead of measuring")
     a = ap.parse_args()
-    x, y, raw = make_dataset(per_mu=a.per_mu, log2n=a.log2n)
+    if a.from_dataset:
+        z = np.load(a.from_dataset)
+        x, y = z["dataset_x"], z["dataset_y"]
+    else:
+        x, y, raw = make_dataset(per_mu=a.per_mu, log2n=a.log2n)
+    y = clip_target(y).astype(np.float32)
     net = WindowMLP(seed=1)
     hist = net.train(x, y, steps=a.steps)
     net.save(a.out, dataset_x=x, dataset_y=y, loss_history=np.array(hist))

@@ -67,6 +67,7 @@ struct Plan {
   // staged stage 1
   int s1fast = 0, JR2 = 0, JT2 = 0, AC = 0, buf_elems = 0;
   int s1_tS = 0;                    // compile-time-S stage-1 instance available
+  int s1_nt = 512;                  // its block size (256: two CTAs per SM)
   size_t smem1b = 0;
   void *d_filt2 = nullptr;          // [d][atap][nmu][S] real
   bool timing = false;
@@ -525,7 +526,7 @@ int staged_jr(int prec, int nmu)
   return nmu == 5 ? 4 : nmu == 3 ? 4 : (nmu == 8 || nmu == 9) ? 2 : 0;
 }
 
-template <typename R, int NMU, int JR, int R0, int R1>
+template <typename R, int NMU, int JR, int R0, int R1, int NT>
 int launch_conv_tS(Plan &p, const void *alpha, void *T, cudaStream_t st)
 {
   Conv2Args a;
@@ -534,27 +535,34 @@ int launch_conv_tS(Plan &p, const void *alpha, void *T, cudaStream_t st)
   a.M = (long long)p.M; a.Mh = (long long)p.Mh; a.J = (long long)p.J;
   a.S = (int)p.S; a.d = p.dmu; a.atap = p.atap; a.JT = p.JT2; a.pitch = p.pitch; a.AC = p.AC;
   a.buf_elems = p.buf_elems;
-  auto kern = k_conv_sfft_tS<R, NMU, JR, R0, R1>;
+  auto kern = k_conv_sfft_tS<R, NMU, JR, R0, R1, NT>;
   CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem1b));
   dim3 grid((unsigned)((p.J + p.JT2 - 1) / p.JT2));
-  kern<<<grid, 512, p.smem1b, st>>>(a);
+  kern<<<grid, NT, p.smem1b, st>>>(a);
   CK(cudaGetLastError());
   return SOI_OK;
 }
 
 // compile-time-S instances: n_mu = 5, S in {8..256} (R0*R1 split of S)
+template <typename R, int JR, int NT>
+int launch_tS_switch_nt(Plan &p, const void *alpha, void *T, cudaStream_t st)
+{
+  switch (p.S) {
+    case 8: return launch_conv_tS<R, 5, JR, 2, 4, NT>(p, alpha, T, st);
+    case 16: return launch_conv_tS<R, 5, JR, 4, 4, NT>(p, alpha, T, st);
+    case 32: return launch_conv_tS<R, 5, JR, 4, 8, NT>(p, alpha, T, st);
+    case 64: return launch_conv_tS<R, 5, JR, 8, 8, NT>(p, alpha, T, st);
+    case 128: return launch_conv_tS<R, 5, JR, 8, 16, NT>(p, alpha, T, st);
+    case 256: return launch_conv_tS<R, 5, JR, 16, 16, NT>(p, alpha, T, st);
+  }
+  return SOI_ERR_UNSUPPORTED;
+}
+
 template <typename R, int JR>
 int launch_tS_switch(Plan &p, const void *alpha, void *T, cudaStream_t st)
 {
-  switch (p.S) {
-    case 8: return launch_conv_tS<R, 5, JR, 2, 4>(p, alpha, T, st);
-    case 16: return launch_conv_tS<R, 5, JR, 4, 4>(p, alpha, T, st);
-    case 32: return launch_conv_tS<R, 5, JR, 4, 8>(p, alpha, T, st);
-    case 64: return launch_conv_tS<R, 5, JR, 8, 8>(p, alpha, T, st);
-    case 128: return launch_conv_tS<R, 5, JR, 8, 16>(p, alpha, T, st);
-    case 256: return launch_conv_tS<R, 5, JR, 16, 16>(p, alpha, T, st);
-  }
-  return SOI_ERR_UNSUPPORTED;
+  return p.s1_nt == 256 ? launch_tS_switch_nt<R, JR, 256>(p, alpha, T, st)
+                        : launch_tS_switch_nt<R, JR, 512>(p, alpha, T, st);
 }
 
 bool tS_available(const Plan &p)
@@ -596,10 +604,14 @@ void plan_stage1_staged(Plan &p)
   if (env_int("SOI_STAGE1_FAST", 1) == 0) return;
   const int jr = staged_jr(p.prec, p.nmu);
   if (!jr || p.S > 512 || (p.S * p.nmu) % 4) return;
-  const int groups = 512 / (int)p.S;
-  const size_t budget = 200 * 1024 - p.S * (p.elem + sizeof(int));
-  const size_t real = p.elem / 2;
   const bool ts = tS_available(p);
+  // compile-time-S kernel: 256 threads and <= 110 KB (two CTAs per SM) where
+  // a tile of at least two thread rows fits, else 512 threads and 200 KB
+  int nt = 512;
+  if (ts && 2 * (int)p.S <= 256) nt = env_int("SOI_STAGE1_NT", 256) == 512 ? 512 : 256;
+  const int groups = nt / (int)p.S;
+  const size_t budget = (nt == 256 ? 110 * 1024 : 200 * 1024) - p.S * (p.elem + sizeof(int));
+  const size_t real = p.elem / 2;
   const size_t pitch = ts ? ((p.S + p.S / tS_r1(p.S)) | 1) : (size_t)p.pitch;
   for (int jt = groups * jr; jt >= jr; jt -= jr) {
     if ((long long)jt > (long long)p.J - p.atap - jt) continue;     // keep the wrap single-step
@@ -615,6 +627,7 @@ void plan_stage1_staged(Plan &p)
         p.smem1b = 2 * be * p.elem + p.S * (p.elem + sizeof(int));
         p.s1fast = 1;
         p.s1_tS = ts ? 1 : 0;
+        p.s1_nt = ts ? nt : 512;
         return;
       }
     }

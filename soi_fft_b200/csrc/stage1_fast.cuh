@@ -196,13 +196,15 @@ template <typename V> struct EmitTransposed {
   }
 };
 
-// Same kernel with the segment count S = R0*R1 known at compile time: shared
+// Same kernel with the segment count S = R0*R1 and the block size NT known at
+// compile time (NT = 256 runs two CTAs per SM, so one CTA's convolution
+// overlaps the other's FFT and stores): shared
 // addressing becomes immediate offsets, and the S-point FFT runs as two
 // register-radix stages (RegDFT) whose last stage writes the transposed
 // output straight to HBM.  Tile layout: row r, column s at
 // r*PITCH + s + s/R1, PITCH odd.
-template <typename R, int NMU, int JR, int R0, int R1>
-__global__ void __launch_bounds__(512, 1) k_conv_sfft_tS(Conv2Args a)
+template <typename R, int NMU, int JR, int R0, int R1, int NT>
+__global__ void __launch_bounds__(NT, 512 / NT) k_conv_sfft_tS(Conv2Args a)
 {
   using V = typename cplx_of<R>::type;
   constexpr int S = R0 * R1;
@@ -227,14 +229,14 @@ __global__ void __launch_bounds__(512, 1) k_conv_sfft_tS(Conv2Args a)
   const V *alpha = reinterpret_cast<const V *>(a.alpha);
   const R *filt = reinterpret_cast<const R *>(a.filt);
   constexpr int CPR = S * (int)sizeof(V) / 16;                // 16-byte chunks per input row
-  static_assert(512 % CPR == 0, "row chunks must tile the block");
+  static_assert(NT % CPR == 0, "row chunks must tile the block");
 
   auto issue = [&](int p, V *dst) {
     const int b = p / nch, a_lo = (p % nch) * a.AC;
     const int n_a = min(a.AC, a.atap - a_lo);
     const int nrows = JT + n_a - 1;
     const int off = tid % CPR;
-    for (int t = tid / CPR; t < nrows; t += 512 / CPR) {
+    for (int t = tid / CPR; t < nrows; t += NT / CPR) {
       long long r = (long long)d * (j0 + a_lo + t) + b;
       if (r >= M) r -= M;                                    // circular (ghost rows, .cpp:495-515)
       cp_async16(reinterpret_cast<char *>(dst + (size_t)t * S) + off * 16,
@@ -243,7 +245,7 @@ __global__ void __launch_bounds__(512, 1) k_conv_sfft_tS(Conv2Args a)
     R *fdst = reinterpret_cast<R *>(dst + (size_t)nrows * S);
     const char *fsrc = reinterpret_cast<const char *>(filt + ((size_t)(b * a.atap + a_lo) * NMU) * S);
     const int fchunks = n_a * NMU * S * (int)sizeof(R) / 16;
-    for (int c = tid; c < fchunks; c += 512) cp_async16(reinterpret_cast<char *>(fdst) + c * 16, fsrc + c * 16);
+    for (int c = tid; c < fchunks; c += NT) cp_async16(reinterpret_cast<char *>(fdst) + c * 16, fsrc + c * 16);
   };
 
   V acc[JR][NMU];

@@ -140,43 +140,51 @@ __device__ __forceinline__ void tile_fft_smem(V *sm, int C, int PP, int PC, cons
 namespace soi {
 
 // tile_fft_smem with the tile geometry known at compile time: C columns,
-// shared index (pos + pos/RL)*PP + col*PC, NT threads.  Column and position
-// come from shifts and constant multiplies instead of runtime divisions.
+// shared index (pos + pos/RL)*PP + col*PC, NT threads.  Every register radix
+// reads and writes its R values at compile-time offsets from one base address
+// (the positions of a butterfly never straddle a pad differently), and the
+// twiddle of the i = 0 butterflies is tw[0] = 1 exactly, so no lane takes a
+// separate path.
 template <typename V, int R0, int R1, int R2, int C, int PP, int PC, int NT, class Emit>
 __device__ __forceinline__ void tile_fft_ct(V *sm, const V *__restrict__ tw, const Emit &emit)
 {
   constexpr int RL = (R2 > 1) ? R2 : R1;
   constexpr int L = R0 * R1 * R2;
   constexpr int span0 = L / R0;
-  auto sidx = [](int col, int pos) { return (pos + pos / RL) * PP + col * PC; };
+  static_assert(span0 % RL == 0, "first-stage stride is a whole number of pad groups");
+  constexpr int D0 = (span0 + span0 / RL) * PP;             // shared distance of span0 positions
+  constexpr int DL = (RL + 1) * PP;                         // shared distance of RL positions
   {
     constexpr int n = C * span0;
 #pragma unroll 1
     for (int q = threadIdx.x; q < n; q += NT) {
       const int col = q % C, i = q / C;
+      V *p = sm + (i + i / RL) * PP + col * PC;
       V v[R0];
 #pragma unroll
-      for (int r = 0; r < R0; ++r) v[r] = sm[sidx(col, i + r * span0)];
+      for (int r = 0; r < R0; ++r) v[r] = p[r * D0];
       RegDFT<V, R0>::run(v);
+      p[0] = v[0];
 #pragma unroll
-      for (int k = 0; k < R0; ++k) sm[sidx(col, i + k * span0)] = (k && i) ? cmul(v[k], tw[i * k]) : v[k];
+      for (int k = 1; k < R0; ++k) p[k * D0] = cmul(v[k], __ldg(tw + i * k));
     }
   }
   __syncthreads();
   if constexpr (R2 > 1) {
-    constexpr int span1 = span0 / R1;
+    constexpr int span1 = span0 / R1;                       // = RL
     constexpr int n = C * (L / R1);
 #pragma unroll 1
     for (int q = threadIdx.x; q < n; q += NT) {
       const int col = q % C, t = q / C;
       const int blk = t / span1, i = t - blk * span1;
-      const int base = blk * span0 + i;
+      V *p = sm + (blk * span0 + blk * (span0 / RL) + i) * PP + col * PC;
       V v[R1];
 #pragma unroll
-      for (int r = 0; r < R1; ++r) v[r] = sm[sidx(col, base + r * span1)];
+      for (int r = 0; r < R1; ++r) v[r] = p[r * DL];
       RegDFT<V, R1>::run(v);
+      p[0] = v[0];
 #pragma unroll
-      for (int k = 0; k < R1; ++k) sm[sidx(col, base + k * span1)] = (k && i) ? cmul(v[k], tw[i * k * R0]) : v[k];
+      for (int k = 1; k < R1; ++k) p[k * DL] = cmul(v[k], __ldg(tw + i * k * R0));
     }
     __syncthreads();
   }
@@ -185,9 +193,10 @@ __device__ __forceinline__ void tile_fft_ct(V *sm, const V *__restrict__ tw, con
 #pragma unroll 1
     for (int q = threadIdx.x; q < n; q += NT) {
       const int col = q % C, blk = q / C;
+      const V *p = sm + blk * DL + col * PC;
       V v[RL];
 #pragma unroll
-      for (int r = 0; r < RL; ++r) v[r] = sm[sidx(col, blk * RL + r)];
+      for (int r = 0; r < RL; ++r) v[r] = p[r * PP];
       RegDFT<V, RL>::run(v);
       int fbase;
       if constexpr (R2 > 1) fbase = (blk / R1) + R0 * (blk % R1);

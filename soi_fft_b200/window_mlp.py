@@ -213,26 +213,40 @@ class WindowMLP:
 
     # ---------------------------------------------------------- proposals --
 
-    def predict_best(self, n_mu, d_mu, ntau=48, nsig=48):
-        """For every B, the (tau, sigma) with the lowest predicted error."""
+    def predict_grid(self, n_mu, d_mu, ntau=48, nsig=48):
+        """Predicted log10 error over the (B, tau, sigma) grid: (Bs, taus, sigmas, pred[B][tau][sigma])."""
         Bs = np.arange(max(B_RANGE[0], d_mu + 1), B_RANGE[1] + 1)
         taus = np.linspace(*TAU_RANGE, ntau)
         sigs = np.exp(np.linspace(np.log(SIGMA_RANGE[0]), np.log(SIGMA_RANGE[1]), nsig))
         BB, TT, SS = np.meshgrid(Bs, taus, sigs, indexing="ij")
         f = features(n_mu, d_mu, BB.ravel(), TT.ravel(), SS.ravel())
         pred = self.forward(f).cpu().numpy().reshape(BB.shape)
-        k = pred.reshape(len(Bs), -1).argmin(1)
+        return Bs, taus, sigs, pred
+
+    def predict_best(self, n_mu, d_mu, ntau=48, nsig=48):
+        """For every B, the (tau, sigma) with the lowest predicted error."""
+        Bs, taus, sigs, pred = self.predict_grid(n_mu, d_mu, ntau, nsig)
         out = []
         for i, b in enumerate(Bs):
-            it, isg = np.unravel_index(k[i], (ntau, nsig))
+            it, isg = np.unravel_index(pred[i].argmin(), pred[i].shape)
             out.append((int(b), float(taus[it]), float(sigs[isg]), float(pred[i, it, isg])))
         return out
 
-    def propose(self, n_mu, d_mu, target, margin=0.5):
-        """Candidates (B, tau, sigma, predicted log10 error) in increasing B
-        whose prediction beats log10(target) by `margin` decades."""
+    def propose(self, n_mu, d_mu, target, slack=0.3, per_b=3):
+        """Candidates (B, tau, sigma, predicted log10 error) in increasing B: for
+        each B the `per_b` best-predicted (tau, sigma) whose prediction is
+        within `slack` decades of the target (the measurement decides)."""
         lt = math.log10(target)
-        return [c for c in self.predict_best(n_mu, d_mu) if c[3] <= lt - margin]
+        Bs, taus, sigs, pred = self.predict_grid(n_mu, d_mu)
+        out = []
+        for i, b in enumerate(Bs):
+            flat = pred[i].ravel()
+            for j in np.argsort(flat)[:per_b]:
+                if flat[j] > lt + slack:
+                    break
+                it, isg = np.unravel_index(j, pred[i].shape)
+                out.append((int(b), float(taus[it]), float(sigs[isg]), float(flat[j])))
+        return out
 
 
 def analytic_window(n_mu, d_mu, target, measure):
@@ -249,7 +263,7 @@ def analytic_window(n_mu, d_mu, target, measure):
     return 72, 928 / 1024., 373.7314, e
 
 
-def learned_window(net, n_mu, d_mu, target, measure, tries=4):
+def learned_window(net, n_mu, d_mu, target, measure, tries=24):
     """A verified proposal: the first candidate (smallest B) whose measured
     error meets the target; None when none of the first `tries` does."""
     for (B, tau, sigma, pred) in net.propose(n_mu, d_mu, target)[:tries]:
@@ -257,6 +271,57 @@ def learned_window(net, n_mu, d_mu, target, measure, tries=4):
         if e <= target:
             return B, tau, sigma, e, pred
     return None
+
+
+def time_transform(x, S, n_mu, d_mu, B, tau, sigma, reps=5):
+    """Median device time (ms) of the FP64 transform with this window."""
+    import torch
+    d = SoiDescriptor(N=x.numel(), n_mu=n_mu, d_mu=d_mu, B=B, tau=float(tau), sigma=float(sigma),
+                      precision=PRECISION_FP64, device=x.device.index or 0)
+    try:
+        d.init(S)
+        y = torch.empty_like(x)
+        d.compute_into(x, y)
+        ts = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a.record()
+            d.compute_into(x, y)
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+    finally:
+        d.free()
+    return float(np.median(ts))
+
+
+def evaluate(net, log2n=26, S=32, targets=(1e-12, 1e-11, 1e-10, 1e-9, 1e-8, 1e-7), seed=1234):
+    """Held-out evaluation: for each oversampling pair and target, the
+    learned (verified) window against the analytic one at N ~ 2^log2n: taps,
+    measured errors and FP64 transform times.  Yields one dict per case."""
+    import torch
+    for (n_mu, d_mu) in MU_PAIRS:
+        N = length_for(n_mu, d_mu, log2n)
+        g = torch.Generator(device="cuda").manual_seed(seed + n_mu)
+        x = torch.complex(torch.randn(N, generator=g, device="cuda", dtype=torch.float64),
+                          torch.randn(N, generator=g, device="cuda", dtype=torch.float64))
+        X = torch.fft.fft(x)
+        measure = lambda B, tau, sigma: measure_error(x, S, n_mu, d_mu, int(B), tau, sigma, X)
+        for tgt in targets:
+            base = analytic_window(n_mu, d_mu, tgt, measure)
+            learned = learned_window(net, n_mu, d_mu, tgt, measure)
+            rec = {"mu": "%d/%d" % (n_mu, d_mu), "N": N, "S": S, "target": tgt,
+                   "analytic": {"B": base[0], "tau": base[1], "sigma": base[2], "err": base[3],
+                                "meets": base[3] <= tgt}}
+            if learned is not None:
+                rec["learned"] = {"B": learned[0], "tau": learned[1], "sigma": learned[2], "err": learned[3],
+                                  "pred": 10 ** learned[4]}
+            if learned is not None and base[3] <= tgt:
+                tb = time_transform(x, S, n_mu, d_mu, *base[:3])
+                tl = time_transform(x, S, n_mu, d_mu, *learned[:3])
+                rec.update(taps_saved=base[0] - learned[0], ms_analytic=tb, ms_learned=tl, speedup=tb / tl)
+            yield rec
 
 
 def main():
@@ -269,7 +334,15 @@ def main():
     ap.add_argument("--out", default=WEIGHTS)
     ap.add_argument("--from-dataset", default=None,
                     help="retrain on the measurements stored in a weights file instead of measuring")
+    ap.add_argument("--evaluate", action="store_true",
+                    help="evaluate the weights in --out against the analytic window instead of training")
+    ap.add_argument("--eval-log2n", type=int, default=26)
     a = ap.parse_args()
+    if a.evaluate:
+        net = WindowMLP.load(a.out)
+        for rec in evaluate(net, log2n=a.eval_log2n):
+            print(json.dumps(rec), flush=True)
+        return
     if a.from_dataset:
         z = np.load(a.from_dataset)
         x, y = z["dataset_x"], z["dataset_y"]

@@ -129,6 +129,10 @@ int soi_plan_geometry(const soi_desc_t *desc, cfft_size_t k, long long *info);
 int soi_last_timings(soi_desc_t *desc, float *ms4);
 /* Enable/disable event timing (off by default). */
 int soi_set_timing(soi_desc_t *desc, int enable);
+/* Number of this library's kernels one compute launches on the device
+ * (stage 1, stage 2, and the VLC round trip when use_vlc is set); < 0 is a
+ * soi_status_t error.  No counterpart in the reference (no GPU there). */
+int soi_kernels_per_compute(soi_desc_t *desc);
 
 /* ---- VLC (compress.c) on the device ------------------------------------ */
 

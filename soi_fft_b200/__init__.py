@@ -67,6 +67,7 @@ def lib():
         L.soi_status_string.restype = ctypes.c_char_p
         L.soi_b200_version.restype = ctypes.c_char_p
         L.soi_set_timing.argtypes = [P, ctypes.c_int]
+        L.soi_kernels_per_compute.argtypes = [P]
         L.soi_last_timings.argtypes = [P, ctypes.POINTER(ctypes.c_float)]
         L.soi_filter_subsample_device.argtypes = [P, ctypes.c_void_p, ctypes.c_void_p]
         L.soi_segment_fft_demod_device.argtypes = [P, ctypes.c_void_p, ctypes.c_void_p]
@@ -202,6 +203,13 @@ class SoiDescriptor:
 
     def set_timing(self, on=True):
         _check(lib().soi_set_timing(ctypes.byref(self._d), int(on)), "soi_set_timing")
+
+    def kernels_per_compute(self):
+        """How many of the library's kernels one compute launches."""
+        n = lib().soi_kernels_per_compute(ctypes.byref(self._d))
+        if n < 0:
+            _check(-n, "soi_kernels_per_compute")
+        return n
 
     def timings(self):
         a = (ctypes.c_float * 4)()

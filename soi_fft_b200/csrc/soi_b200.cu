@@ -1087,6 +1087,15 @@ int soi_plan_geometry(const soi_desc_t *d, cfft_size_t k, long long *info)
   return SOI_OK;
 }
 
+int soi_kernels_per_compute(soi_desc_t *d)
+{
+  Plan *p = plan_of(d);
+  if (!p) return -SOI_ERR_NOT_INITIALISED;
+  int n = 1 + (p->fast2 ? 1 : 2);
+  if (d->use_vlc) n += p->prec == SOI_PRECISION_FP64 ? 4 : 6;   // run_vlc
+  return n;
+}
+
 int soi_set_timing(soi_desc_t *d, int enable)
 {
   Plan *p = plan_of(d);

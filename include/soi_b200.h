@@ -101,6 +101,23 @@ int soi_compute_status(soi_desc_t *desc, void *alpha_dt);
  * receives the N outputs; both host or both device memory per device_ptr.
  * No counterpart in the reference, whose compute_soi is in-place only. */
 int soi_compute_oop_status(soi_desc_t *desc, const void *in, void *out);
+/* Segments of interest: the outputs of segments [seg_lo, seg_hi) only
+ * (out[seg_lo*M .. seg_hi*M), M = N/k); the rest of `out` is left as it was.
+ * The convolution still reads all N inputs, but the transposed store, the
+ * M'-point FFTs and the demodulation run for those segments only, so a band
+ * of the spectrum costs its share of stage 2.  Results are bit-identical to
+ * the same segments of a full compute.  Host or device buffers per
+ * device_ptr.  No counterpart in the reference, where each rank computes the
+ * segments it owns (pfft.c:584-694). */
+int soi_compute_segments_status(soi_desc_t *desc, const void *in, void *out, int seg_lo, int seg_hi);
+/* Out-of-place compute on device buffers (device_ptr = 1) that only enqueues
+ * work on the descriptor's stream and never waits on it, so it can be
+ * recorded into a CUDA graph.  A persistent-kernel wait that gave up is
+ * reported by the next soi_check_status.  No counterpart in the reference. */
+int soi_compute_async_status(soi_desc_t *desc, const void *in, void *out);
+/* Waits for the descriptor's stream and returns SOI_ERR_TIMEOUT if a
+ * stage-2 dependency wait gave up since the last compute, else SOI_OK. */
+int soi_check_status(soi_desc_t *desc);
 int soi_filter_subsampling_status(soi_desc_t *desc, void *alpha_dt);
 int soi_free_status(soi_desc_t *desc);
 const char *soi_status_string(int status);

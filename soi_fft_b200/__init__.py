@@ -62,6 +62,9 @@ def lib():
         for name in ("soi_compute_status", "soi_filter_subsampling_status", "soi_get_transposed"):
             getattr(L, name).argtypes = [P, ctypes.c_void_p]
         L.soi_compute_oop_status.argtypes = [P, ctypes.c_void_p, ctypes.c_void_p]
+        L.soi_compute_segments_status.argtypes = [P, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        L.soi_compute_async_status.argtypes = [P, ctypes.c_void_p, ctypes.c_void_p]
+        L.soi_check_status.argtypes = [P]
         L.soi_free_status.argtypes = [P]
         L.set_default_soi_descriptor.argtypes = [P]
         L.soi_status_string.restype = ctypes.c_char_p
@@ -187,6 +190,32 @@ class SoiDescriptor:
             raise ValueError("x and out must both be host arrays or both CUDA tensors")
         _check(lib().soi_compute_oop_status(ctypes.byref(self._d), px, po), "soi_compute_oop")
         return out
+
+    def compute_segments(self, x, out, seg_lo, seg_hi):
+        """Segments of interest: outputs of segments [seg_lo, seg_hi) only
+        (out[seg_lo*M : seg_hi*M]); the rest of out is left as it was."""
+        px = self._ptr(x)
+        dev = self._d.device_ptr
+        po = self._ptr(out)
+        if self._d.device_ptr != dev:
+            raise ValueError("x and out must both be host arrays or both CUDA tensors")
+        _check(lib().soi_compute_segments_status(ctypes.byref(self._d), px, po, int(seg_lo), int(seg_hi)),
+               "soi_compute_segments")
+        return out
+
+    def compute_async(self, x, out):
+        """Enqueue the transform of CUDA tensors x -> out on the descriptor's
+        stream without waiting (capturable); check() reports a stage-2 wait
+        that gave up."""
+        if not (_is_torch_cuda(x) and _is_torch_cuda(out)):
+            raise ValueError("compute_async takes CUDA tensors")
+        px, po = self._ptr(x), self._ptr(out)
+        _check(lib().soi_compute_async_status(ctypes.byref(self._d), px, po), "soi_compute_async")
+        return out
+
+    def check(self):
+        """Wait for the descriptor's stream; raise if a stage-2 wait gave up."""
+        _check(lib().soi_check_status(ctypes.byref(self._d)), "soi_check_status")
 
     def filter_subsampling(self, x):
         """parallel_filter_subsampling (.cpp:535): stage 1 only; returns the

@@ -49,19 +49,16 @@ struct Plan {
   double *d_vlc_x = nullptr;   // promoted/decompressed doubles (FP32 path)
   int *d_vlc_words = nullptr, *d_vlc_n = nullptr, *d_vlc_emax = nullptr;
   long vlc_stride = 0;
-  // persistent stage 2 (split form): compiled radix split and its state
-  int fast2 = 0;               // 0: two-kernel stage 2, 1: runtime-geometry persistent kernel,
-                               // 3: compile-time-geometry persistent kernel (2, 4: chosen, not set up)
+  // persistent stage 2: compiled radix split and its state
+  int fast2 = 0;               // 0: two-kernel stage 2, 3: persistent kernel (4: chosen, not set up)
   int f2_variant = 0;
   int f2_grid = 0;
   size_t f2_smem = 0;
-  int f2_ps2 = 0;
-  int f2_buf = 0;
+  int discard = 1;             // drop consumed intermediate lines from L2
   void *d_amp = nullptr;            // [M/2+1] real demodulation amplitude
   double2 *d_dlo = nullptr, *d_dhi = nullptr;
   int dlo_bits = 11;
-  void (*f2_kernel)(S2Args) = nullptr;
-  void (*f2ct_kernel)(S2ArgsCT) = nullptr;   // compile-time-geometry stage 2 (fast2 == 3)
+  void (*f2ct_kernel)(S2ArgsCT) = nullptr;
   void *d_ph2 = nullptr;            // [M2] complex exp(-i pi kappa M1 k2 / M)
   unsigned int *d_sync = nullptr;   // [0] counter, [1] err, [2..2+S) done1
   // staged stage 1
@@ -73,6 +70,19 @@ struct Plan {
   bool timing = false;
   cudaEvent_t ev[5] = {};
   float ms[4] = {0, 0, 0, 0};
+};
+
+// One execution of the transform (or of a band of its segments): device
+// buffers, stage-2 synchronisation words and the stream.  A plan's own
+// compute uses the plan's scratch; the batch driver gives each concurrent
+// chain its own.
+struct Exec {
+  const void *in;              // N inputs [M rows][S]
+  void *T;                     // S x M' transposed data
+  void *out;                   // N outputs [S][M] (rows of segments outside [lo, hi) untouched)
+  unsigned int *sync;          // [0] task counter, [1] error flag, [2 .. 2 + S) pass-1 counts
+  int lo, hi;                  // segments computed
+  cudaStream_t st;
 };
 
 #define CK(x)                                                                    \
@@ -217,31 +227,30 @@ int upload(void **dst, const void *src, size_t bytes)
 // ---- kernel dispatch ---------------------------------------------------------
 
 template <typename R, int NMU, int JR>
-int launch_conv_t(Plan &p, const void *alpha, void *T, cudaStream_t st)
+int launch_conv_t(Plan &p, const Exec &ex)
 {
   ConvArgs a;
-  a.alpha = alpha; a.T = T; a.filt = p.d_filt; a.phase = p.d_phase; a.twS = p.d_twS;
+  a.alpha = ex.in; a.T = ex.T; a.filt = p.d_filt; a.seg_lo = ex.lo; a.seg_hi = ex.hi; a.phase = p.d_phase; a.twS = p.d_twS;
   a.permS = p.d_permS; a.wsmall = p.d_wsmall; a.planS = p.planS;
   a.M = (long long)p.M; a.Mh = (long long)p.Mh; a.J = (long long)p.J;
   a.S = (int)p.S; a.d = p.dmu; a.atap = p.atap; a.JT = p.JT; a.pitch = p.pitch;
   auto kern = k_conv_sfft<R, NMU, JR>;
   CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem1));
   dim3 grid((unsigned)((p.J + p.JT - 1) / p.JT));
-  kern<<<grid, 256, p.smem1, st>>>(a);
+  kern<<<grid, 256, p.smem1, ex.st>>>(a);
   CK(cudaGetLastError());
   return SOI_OK;
 }
 
 template <typename R>
-int launch_conv_r(Plan &p, const void *alpha, void *T, cudaStream_t st)
+int launch_conv_r(Plan &p, const Exec &ex)
 {
-  const bool big = sizeof(R) == 8;
   switch (p.nmu) {
-    case 2: return big ? launch_conv_t<R, 2, 8>(p, alpha, T, st) : launch_conv_t<R, 2, 8>(p, alpha, T, st);
-    case 3: return launch_conv_t<R, 3, 8>(p, alpha, T, st);
-    case 5: return launch_conv_t<R, 5, 8>(p, alpha, T, st);
-    case 8: return launch_conv_t<R, 8, 4>(p, alpha, T, st);
-    case 9: return launch_conv_t<R, 9, 4>(p, alpha, T, st);
+    case 2: return launch_conv_t<R, 2, 8>(p, ex);
+    case 3: return launch_conv_t<R, 3, 8>(p, ex);
+    case 5: return launch_conv_t<R, 5, 8>(p, ex);
+    case 8: return launch_conv_t<R, 8, 4>(p, ex);
+    case 9: return launch_conv_t<R, 9, 4>(p, ex);
     default: return SOI_ERR_UNSUPPORTED;
   }
 }
@@ -250,10 +259,11 @@ int jr_for(int nmu) { return nmu >= 8 ? 4 : 8; }
 bool nmu_supported(int nmu) { return nmu == 2 || nmu == 3 || nmu == 5 || nmu == 8 || nmu == 9; }
 
 template <typename R>
-int launch_seg_t(Plan &p, void *T, void *out, cudaStream_t st)
+int launch_seg_t(Plan &p, const Exec &ex)
 {
   SegArgs a;
-  a.T = T; a.out = out;
+  a.T = ex.T; a.out = ex.out; a.seg_lo = ex.lo;
+  cudaStream_t st = ex.st;
   a.tw1 = p.d_tw1; a.perm1 = p.d_perm1; a.plan1 = p.plan1;
   a.tw2 = p.d_tw2; a.perm2 = p.d_perm2; a.plan2 = p.plan2;
   a.xtw_lo = p.d_xlo; a.xtw_hi = p.d_xhi; a.winv = p.d_winv; a.wsmall = p.d_wsmall;
@@ -261,50 +271,13 @@ int launch_seg_t(Plan &p, void *T, void *out, cudaStream_t st)
   a.M1 = p.M1; a.M2 = p.M2; a.C1 = p.C1; a.C2 = p.C2; a.lo_bits = p.lo_bits;
   CK(cudaFuncSetAttribute(k_seg_cols<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_c));
   CK(cudaFuncSetAttribute(k_seg_rows_demod<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_r));
-  dim3 g1((unsigned)(p.M2 / p.C1), (unsigned)p.S);
+  dim3 g1((unsigned)(p.M2 / p.C1), (unsigned)(ex.hi - ex.lo));
   k_seg_cols<R><<<g1, 256, p.smem_c, st>>>(a);
   CK(cudaGetLastError());
-  dim3 g2((unsigned)(p.M1 / p.C2), (unsigned)p.S);
+  dim3 g2((unsigned)(p.M1 / p.C2), (unsigned)(ex.hi - ex.lo));
   k_seg_rows_demod<R><<<g2, 256, p.smem_r, st>>>(a);
   CK(cudaGetLastError());
   return SOI_OK;
-}
-
-// ---- persistent stage 2 -------------------------------------------------------
-
-using S2Kernel = void (*)(S2Args);
-
-struct S2Choice { int M1, M2, r0, r1, r2, q0, q1, q2; S2Kernel k; };
-
-// compiled splits (split form): M1 = r0*r1*r2, M2 = q0*q1*q2
-const S2Choice kS2Choices[] = {
-  { 2560, 2048, 10, 16, 16, 8, 16, 16, k_stage2_persistent<float, 10, 16, 16, 8, 16, 16> },
-  { 2560, 2048, 40, 64, 1, 32, 64, 1, k_stage2_persistent<float, 40, 64, 1, 32, 64, 1> },
-  { 2560, 1024, 10, 16, 16, 4, 16, 16, k_stage2_persistent<float, 10, 16, 16, 4, 16, 16> },
-  { 1280, 1024, 5, 16, 16, 4, 16, 16, k_stage2_persistent<float, 5, 16, 16, 4, 16, 16> },
-  { 1280, 512, 5, 16, 16, 8, 8, 8, k_stage2_persistent<float, 5, 16, 16, 8, 8, 8> },
-  { 640, 1024, 10, 8, 8, 4, 16, 16, k_stage2_persistent<float, 10, 8, 8, 4, 16, 16> },
-  { 640, 512, 10, 8, 8, 8, 8, 8, k_stage2_persistent<float, 10, 8, 8, 8, 8, 8> },
-  { 320, 512, 5, 8, 8, 8, 8, 8, k_stage2_persistent<float, 5, 8, 8, 8, 8, 8> },
-  { 320, 256, 5, 8, 8, 4, 8, 8, k_stage2_persistent<float, 5, 8, 8, 4, 8, 8> },
-};
-
-// Select a compiled persistent split for M' (split form only); returns the
-// index into kS2Choices or -1.  Three-stage register splits are preferred;
-// SOI_STAGE2_VARIANT=2 selects the two-stage (radix-64) one where compiled.
-int pick_fast2(const Plan &p)
-{
-  if (p.prec != SOI_PRECISION_SPLIT_FP32 || env_int("SOI_STAGE2_FAST", 1) == 0 ||
-      env_int("SOI_STAGE2_KERNEL", 3) != 2) return -1;
-  const bool want2 = env_int("SOI_STAGE2_VARIANT", 0) == 2;
-  int best = -1;
-  for (int i = 0; i < (int)(sizeof(kS2Choices) / sizeof(kS2Choices[0])); ++i) {
-    const S2Choice &c = kS2Choices[i];
-    if ((long long)c.M1 * c.M2 != (long long)p.Mh) continue;
-    const bool two = c.r2 == 1;
-    if (best < 0 || (two == want2 && (kS2Choices[best].r2 == 1) != want2)) best = i;
-  }
-  return best;
 }
 
 // Register-DFT twiddles in constant memory (long double, rounded once).
@@ -360,10 +333,8 @@ const S2ChoiceCT kS2CT[] = {
 // index into kS2CT for M' and the element size, or -1
 int pick_s2ct(const Plan &p)
 {
-  // SOI_STAGE2_KERNEL: 3 this kernel (default), 2 the runtime-geometry
-  // persistent kernel, 1 the two-kernel path; SOI_STAGE2_FAST=0 also selects
-  // the two-kernel path
-  if (env_int("SOI_STAGE2_KERNEL", 3) != 3 || env_int("SOI_STAGE2_FAST", 1) == 0) return -1;
+  // SOI_STAGE2_FAST=0 selects the two-kernel path
+  if (env_int("SOI_STAGE2_FAST", 1) == 0) return -1;
   for (int i = 0; i < (int)(sizeof(kS2CT) / sizeof(kS2CT[0])); ++i)
     if ((long long)kS2CT[i].M1 * kS2CT[i].M2 == (long long)p.Mh && kS2CT[i].elem == (int)p.elem) return i;
   return -1;
@@ -427,86 +398,42 @@ int setup_s2ct(Plan &p, int idx)
   CK(cudaMalloc(&p.d_sync, (p.S + 2) * sizeof(unsigned int)));
   int rc = p.prec == SOI_PRECISION_FP64 ? build_demod_tables<double>(p, true) : build_demod_tables<float>(p, true);
   if (rc) return rc;
+  p.discard = env_int("SOI_STAGE2_DISCARD", 1);
   p.fast2 = 3;
   return SOI_OK;
 }
 
-int launch_s2ct(Plan &p, void *T, void *out, cudaStream_t st)
+int launch_s2ct(Plan &p, const Exec &ex)
 {
   S2ArgsCT a;
-  a.T = T; a.out = out; a.tw1 = p.d_tw1; a.tw2 = p.d_tw2; a.xlo = p.d_xlo; a.xhi = p.d_xhi;
+  a.T = ex.T; a.out = ex.out; a.tw1 = p.d_tw1; a.tw2 = p.d_tw2; a.xlo = p.d_xlo; a.xhi = p.d_xhi;
   a.amp = p.d_amp; a.dlo = p.d_dlo; a.dhi = p.d_dhi; a.ph2 = p.d_ph2;
-  a.lo_bits = p.lo_bits; a.dlo_bits = p.dlo_bits; a.M = (int)p.M; a.S = (int)p.S;
-  a.discard = env_int("SOI_STAGE2_DISCARD", 1);
-  a.counter = p.d_sync; a.err = (int *)(p.d_sync + 1); a.done1 = p.d_sync + 2;
-  CK(cudaMemsetAsync(p.d_sync, 0, (p.S + 2) * sizeof(unsigned int), st));
-  p.f2ct_kernel<<<p.f2_grid, 256, p.f2_smem, st>>>(a);
+  a.lo_bits = p.lo_bits; a.dlo_bits = p.dlo_bits; a.M = (int)p.M;
+  a.S = ex.hi - ex.lo; a.seg_lo = ex.lo;
+  a.discard = p.discard;
+  a.counter = ex.sync; a.err = (int *)(ex.sync + 1); a.done1 = ex.sync + 2;
+  CK(cudaMemsetAsync(ex.sync, 0, (size_t)(a.S + 2) * sizeof(unsigned int), ex.st));
+  p.f2ct_kernel<<<p.f2_grid, 256, p.f2_smem, ex.st>>>(a);
   CK(cudaGetLastError());
   return SOI_OK;
 }
 
-int setup_fast2(Plan &p, int idx)
+// Error flag of the persistent stage-2 kernel (a dependency wait that gave
+// up); synchronises the stream.
+int check_stage2(Plan &p, const unsigned int *sync, cudaStream_t st)
 {
-  const S2Choice &c = kS2Choices[idx];
-  p.M1 = c.M1; p.M2 = c.M2;
-  p.C1 = 2; p.C2 = 2;                      // 16-byte column runs; neighbouring tiles share sectors in L2
-  const int RLa = c.r2 > 1 ? c.r2 : c.r1, RLb = c.q2 > 1 ? c.q2 : c.q1;
-  const size_t smA = (size_t)(p.M1 + p.M1 / RLa) * p.C1;
-  int ps2 = p.M2 + p.M2 / RLb;
-  while (ps2 % 16 != 8) ++ps2;             // pass-2 columns 16 words apart in the banks
-  p.f2_ps2 = ps2;
-  const size_t smB = (size_t)ps2 * p.C2;
-  size_t be = std::max(smA, smB);
-  be += be & 1;
-  p.f2_buf = (int)be;
-  p.f2_smem = be * p.elem;
-  p.f2_kernel = c.k;
-  CK(cudaFuncSetAttribute(c.k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.f2_smem));
-  int occ = 0, nsm = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, c.k, 128, p.f2_smem));
-  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, p.device));
-  if (occ < 1) return SOI_ERR_UNSUPPORTED;
-  p.f2_grid = occ * nsm;
-  CK(cudaMalloc(&p.d_sync, (p.S + 2) * sizeof(unsigned int)));
-  // demodulation W_inv[k] = exp(-i pi kappa k/M) * amp[k] (pfft.c:68-82)
-  {
-    int rc = build_demod_tables<float>(p, false);
-    if (rc) return rc;
-  }
-  p.fast2 = 1;
-  return SOI_OK;
-}
-
-int launch_fast2(Plan &p, void *T, void *out, cudaStream_t st)
-{
-  S2Args a;
-  a.T = T; a.out = out; a.tw1 = p.d_tw1; a.tw2 = p.d_tw2; a.xlo = p.d_xlo; a.xhi = p.d_xhi;
-  a.winv = p.d_winv; a.Mh = (long long)p.Mh; a.M = (long long)p.M;
-  a.M1 = p.M1; a.M2 = p.M2; a.C1 = p.C1; a.C2 = p.C2; a.S = (int)p.S; a.lo_bits = p.lo_bits;
-  a.nt1 = p.M2 / p.C1; a.nt2 = p.M1 / p.C2; a.ps2 = p.f2_ps2;
-  a.discard = env_int("SOI_STAGE2_DISCARD", 1);
-  a.amp = p.d_amp; a.dlo = p.d_dlo; a.dhi = p.d_dhi; a.dlo_bits = p.dlo_bits; a.buf_elems = p.f2_buf;
-  a.counter = p.d_sync; a.err = (int *)(p.d_sync + 1); a.done1 = p.d_sync + 2;
-  CK(cudaMemsetAsync(p.d_sync, 0, (p.S + 2) * sizeof(unsigned int), st));
-  p.f2_kernel<<<p.f2_grid, 128, p.f2_smem, st>>>(a);
-  CK(cudaGetLastError());
-  return SOI_OK;
-}
-
-int check_fast2(Plan &p, cudaStream_t st)
-{
-  if (!p.fast2) return SOI_OK;
+  if (!p.fast2 || !sync) return SOI_OK;
   int err = 0;
-  CK(cudaMemcpyAsync(&err, p.d_sync + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(&err, sync + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   return err ? SOI_ERR_TIMEOUT : SOI_OK;
 }
 
 template <typename R, int NMU, int JR>
-int launch_conv2_t(Plan &p, const void *alpha, void *T, cudaStream_t st)
+int launch_conv2_t(Plan &p, const Exec &ex)
 {
   Conv2Args a;
-  a.alpha = alpha; a.T = T; a.filt = p.d_filt2; a.phase = p.d_phase; a.twS = p.d_twS;
+  a.alpha = ex.in; a.T = ex.T; a.seg_lo = ex.lo; a.seg_hi = ex.hi; a.filt = p.d_filt2; a.phase = p.d_phase; a.twS = p.d_twS;
   a.permS = p.d_permS; a.wsmall = p.d_wsmall; a.planS = p.planS;
   a.M = (long long)p.M; a.Mh = (long long)p.Mh; a.J = (long long)p.J;
   a.S = (int)p.S; a.d = p.dmu; a.atap = p.atap; a.JT = p.JT2; a.pitch = p.pitch; a.AC = p.AC;
@@ -514,7 +441,7 @@ int launch_conv2_t(Plan &p, const void *alpha, void *T, cudaStream_t st)
   auto kern = k_conv_sfft_staged<R, NMU, JR>;
   CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem1b));
   dim3 grid((unsigned)((p.J + p.JT2 - 1) / p.JT2));
-  kern<<<grid, 512, p.smem1b, st>>>(a);
+  kern<<<grid, 512, p.smem1b, ex.st>>>(a);
   CK(cudaGetLastError());
   return SOI_OK;
 }
@@ -527,10 +454,10 @@ int staged_jr(int prec, int nmu)
 }
 
 template <typename R, int NMU, int JR, int R0, int R1, int NT>
-int launch_conv_tS(Plan &p, const void *alpha, void *T, cudaStream_t st)
+int launch_conv_tS(Plan &p, const Exec &ex)
 {
   Conv2Args a;
-  a.alpha = alpha; a.T = T; a.filt = p.d_filt2; a.phase = p.d_phase; a.twS = p.d_twS;
+  a.alpha = ex.in; a.T = ex.T; a.seg_lo = ex.lo; a.seg_hi = ex.hi; a.filt = p.d_filt2; a.phase = p.d_phase; a.twS = p.d_twS;
   a.permS = p.d_permS; a.wsmall = p.d_wsmall; a.planS = p.planS;
   a.M = (long long)p.M; a.Mh = (long long)p.Mh; a.J = (long long)p.J;
   a.S = (int)p.S; a.d = p.dmu; a.atap = p.atap; a.JT = p.JT2; a.pitch = p.pitch; a.AC = p.AC;
@@ -538,31 +465,30 @@ int launch_conv_tS(Plan &p, const void *alpha, void *T, cudaStream_t st)
   auto kern = k_conv_sfft_tS<R, NMU, JR, R0, R1, NT>;
   CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem1b));
   dim3 grid((unsigned)((p.J + p.JT2 - 1) / p.JT2));
-  kern<<<grid, NT, p.smem1b, st>>>(a);
+  kern<<<grid, NT, p.smem1b, ex.st>>>(a);
   CK(cudaGetLastError());
   return SOI_OK;
 }
 
 // compile-time-S instances: n_mu = 5, S in {8..256} (R0*R1 split of S)
 template <typename R, int JR, int NT>
-int launch_tS_switch_nt(Plan &p, const void *alpha, void *T, cudaStream_t st)
+int launch_tS_switch_nt(Plan &p, const Exec &ex)
 {
   switch (p.S) {
-    case 8: return launch_conv_tS<R, 5, JR, 2, 4, NT>(p, alpha, T, st);
-    case 16: return launch_conv_tS<R, 5, JR, 4, 4, NT>(p, alpha, T, st);
-    case 32: return launch_conv_tS<R, 5, JR, 4, 8, NT>(p, alpha, T, st);
-    case 64: return launch_conv_tS<R, 5, JR, 8, 8, NT>(p, alpha, T, st);
-    case 128: return launch_conv_tS<R, 5, JR, 8, 16, NT>(p, alpha, T, st);
-    case 256: return launch_conv_tS<R, 5, JR, 16, 16, NT>(p, alpha, T, st);
+    case 8: return launch_conv_tS<R, 5, JR, 2, 4, NT>(p, ex);
+    case 16: return launch_conv_tS<R, 5, JR, 4, 4, NT>(p, ex);
+    case 32: return launch_conv_tS<R, 5, JR, 4, 8, NT>(p, ex);
+    case 64: return launch_conv_tS<R, 5, JR, 8, 8, NT>(p, ex);
+    case 128: return launch_conv_tS<R, 5, JR, 8, 16, NT>(p, ex);
+    case 256: return launch_conv_tS<R, 5, JR, 16, 16, NT>(p, ex);
   }
   return SOI_ERR_UNSUPPORTED;
 }
 
 template <typename R, int JR>
-int launch_tS_switch(Plan &p, const void *alpha, void *T, cudaStream_t st)
+int launch_tS_switch(Plan &p, const Exec &ex)
 {
-  return p.s1_nt == 256 ? launch_tS_switch_nt<R, JR, 256>(p, alpha, T, st)
-                        : launch_tS_switch_nt<R, JR, 512>(p, alpha, T, st);
+  return p.s1_nt == 256 ? launch_tS_switch_nt<R, JR, 256>(p, ex) : launch_tS_switch_nt<R, JR, 512>(p, ex);
 }
 
 bool tS_available(const Plan &p)
@@ -574,24 +500,24 @@ bool tS_available(const Plan &p)
 // last radix of the compile-time-S split (the tile layout pads every R1)
 int tS_r1(size_t S) { return S == 8 ? 4 : S == 16 ? 4 : S == 32 ? 8 : S == 64 ? 8 : 16; }
 
-int launch_conv2(Plan &p, const void *alpha, void *T, cudaStream_t st)
+int launch_conv2(Plan &p, const Exec &ex)
 {
   if (p.s1_tS)
-    return p.prec == SOI_PRECISION_SPLIT_FP32 ? launch_tS_switch<float, 6>(p, alpha, T, st)
-                                              : launch_tS_switch<double, 4>(p, alpha, T, st);
+    return p.prec == SOI_PRECISION_SPLIT_FP32 ? launch_tS_switch<float, 6>(p, ex)
+                                              : launch_tS_switch<double, 4>(p, ex);
   if (p.prec == SOI_PRECISION_SPLIT_FP32) {
     switch (p.nmu) {
-      case 5: return launch_conv2_t<float, 5, 6>(p, alpha, T, st);
-      case 3: return launch_conv2_t<float, 3, 6>(p, alpha, T, st);
-      case 8: return launch_conv2_t<float, 8, 4>(p, alpha, T, st);
-      case 9: return launch_conv2_t<float, 9, 4>(p, alpha, T, st);
+      case 5: return launch_conv2_t<float, 5, 6>(p, ex);
+      case 3: return launch_conv2_t<float, 3, 6>(p, ex);
+      case 8: return launch_conv2_t<float, 8, 4>(p, ex);
+      case 9: return launch_conv2_t<float, 9, 4>(p, ex);
     }
   } else {
     switch (p.nmu) {
-      case 5: return launch_conv2_t<double, 5, 4>(p, alpha, T, st);
-      case 3: return launch_conv2_t<double, 3, 4>(p, alpha, T, st);
-      case 8: return launch_conv2_t<double, 8, 2>(p, alpha, T, st);
-      case 9: return launch_conv2_t<double, 9, 2>(p, alpha, T, st);
+      case 5: return launch_conv2_t<double, 5, 4>(p, ex);
+      case 3: return launch_conv2_t<double, 3, 4>(p, ex);
+      case 8: return launch_conv2_t<double, 8, 2>(p, ex);
+      case 9: return launch_conv2_t<double, 9, 2>(p, ex);
     }
   }
   return SOI_ERR_UNSUPPORTED;
@@ -634,22 +560,19 @@ void plan_stage1_staged(Plan &p)
   }
 }
 
-int run_stage1(Plan &p, const void *alpha, void *T, cudaStream_t st)
+int run_stage1(Plan &p, const Exec &ex)
 {
-  if (p.s1fast) return launch_conv2(p, alpha, T, st);
-  return p.prec == SOI_PRECISION_FP64 ? launch_conv_r<double>(p, alpha, T, st)
-                                      : launch_conv_r<float>(p, alpha, T, st);
+  if (p.s1fast) return launch_conv2(p, ex);
+  return p.prec == SOI_PRECISION_FP64 ? launch_conv_r<double>(p, ex) : launch_conv_r<float>(p, ex);
 }
 
-int run_stage2(Plan &p, void *T, void *out, cudaStream_t st)
+int run_stage2(Plan &p, const Exec &ex)
 {
-  if (p.fast2 == 3) return launch_s2ct(p, T, out, st);
-  if (p.fast2) return launch_fast2(p, T, out, st);
-  return p.prec == SOI_PRECISION_FP64 ? launch_seg_t<double>(p, T, out, st)
-                                      : launch_seg_t<float>(p, T, out, st);
+  if (p.fast2) return launch_s2ct(p, ex);
+  return p.prec == SOI_PRECISION_FP64 ? launch_seg_t<double>(p, ex) : launch_seg_t<float>(p, ex);
 }
 
-int run_vlc(Plan &p, void *T, cudaStream_t st);
+int run_vlc(Plan &p, const Exec &ex);
 
 // ---- plan construction -------------------------------------------------------
 
@@ -810,17 +733,6 @@ int plan_geometry(const soi_desc_t *d, size_t k, Plan &p)
     make_fft_plan(p.M2, p.plan2);
     return SOI_OK;
   }
-  int idx = pick_fast2(p);
-  if (idx >= 0) {
-    p.f2_variant = idx;
-    p.M1 = kS2Choices[idx].M1;
-    p.M2 = kS2Choices[idx].M2;
-    p.C1 = p.C2 = 2;
-    p.fast2 = 2;                 // chosen; set up when the device plan is built
-    make_fft_plan(p.M1, p.plan1);
-    make_fft_plan(p.M2, p.plan2);
-    return SOI_OK;
-  }
   return choose_split(p);
 }
 
@@ -834,10 +746,7 @@ int init_plan(soi_desc_t *d, size_t k)
   rc = p->prec == SOI_PRECISION_FP64 ? build_tables<double>(*p) : build_tables<float>(*p);
   if (rc) { free_plan(p); return rc; }
   if ((rc = upload_regtw())) { free_plan(p); return rc; }
-  if (p->fast2 == 2) {
-    p->fast2 = 0;
-    if ((rc = setup_fast2(*p, p->f2_variant))) { free_plan(p); return rc; }
-  } else if (p->fast2 == 4) {
+  if (p->fast2 == 4) {
     p->fast2 = 0;
     if ((rc = setup_s2ct(*p, p->f2_variant))) { free_plan(p); return rc; }
   }
@@ -858,10 +767,18 @@ Plan *plan_of(soi_desc_t *d) { return d ? (Plan *)d->plan : nullptr; }
 
 // One transform: in -> out (they may alias, the reference's in-place form).
 // Host pointers are staged through the plan's device buffer.
-int compute_impl(soi_desc_t *d, const void *in, void *out, bool stage1_only)
+// The transform of `in` into `out` for segments [seg_lo, seg_hi).  With
+// sync_after false the work is only enqueued (nothing waits on the stream,
+// so it can be captured into a CUDA graph); soi_check_status reads the
+// stage-2 error flag afterwards.
+int compute_impl(soi_desc_t *d, const void *in, void *out, bool stage1_only, int seg_lo = 0, int seg_hi = -1,
+                 bool sync_after = true)
 {
   Plan *p = plan_of(d);
   if (!p) return SOI_ERR_NOT_INITIALISED;
+  if (seg_hi < 0) seg_hi = (int)p->S;
+  if (seg_lo < 0 || seg_hi > (int)p->S || seg_lo >= seg_hi) return SOI_ERR_INVALID;
+  if (!sync_after && !d->device_ptr) return SOI_ERR_INVALID;     // host buffers need the copies to finish
   if (cudaSetDevice(p->device) != cudaSuccess) return SOI_ERR_CUDA;
   cudaStream_t st = p->stream;
   const size_t bytes = p->N * p->elem;
@@ -874,20 +791,28 @@ int compute_impl(soi_desc_t *d, const void *in, void *out, bool stage1_only)
     dst = p->d_io;
   }
   int rc;
+  const Exec ex{ src, p->d_T, dst, p->d_sync, seg_lo, seg_hi, st };
   if (p->timing) CK(cudaEventRecord(p->ev[0], st));
-  if ((rc = run_stage1(*p, src, p->d_T, st))) return rc;
+  if ((rc = run_stage1(*p, ex))) return rc;
   if (p->timing) CK(cudaEventRecord(p->ev[1], st));
   if (stage1_only) {
+    if (!sync_after) return SOI_OK;
     CK(cudaStreamSynchronize(st));
     return SOI_OK;
   }
-  if (d->use_vlc && (rc = run_vlc(*p, p->d_T, st))) return rc;
+  if (d->use_vlc && (rc = run_vlc(*p, ex))) return rc;
   if (p->timing) CK(cudaEventRecord(p->ev[2], st));
-  if ((rc = run_stage2(*p, p->d_T, dst, st))) return rc;
+  if ((rc = run_stage2(*p, ex))) return rc;
   if (p->timing) CK(cudaEventRecord(p->ev[3], st));
-  if (!d->device_ptr) CK(cudaMemcpyAsync(out, p->d_io, bytes, cudaMemcpyDeviceToHost, st));
+  if (!d->device_ptr) {
+    // only the computed segments are copied back
+    const size_t seg_bytes = p->M * p->elem;
+    CK(cudaMemcpyAsync((char *)out + seg_lo * seg_bytes, (const char *)p->d_io + seg_lo * seg_bytes,
+                       (size_t)(seg_hi - seg_lo) * seg_bytes, cudaMemcpyDeviceToHost, st));
+  }
+  if (!sync_after) return SOI_OK;
   CK(cudaStreamSynchronize(st));
-  if ((rc = check_fast2(*p, st))) return rc;
+  if ((rc = check_stage2(*p, p->d_sync, st))) return rc;
   if (p->timing) {
     cudaEventElapsedTime(&p->ms[0], p->ev[0], p->ev[1]);
     cudaEventElapsedTime(&p->ms[2], p->ev[1], p->ev[2]);
@@ -901,17 +826,21 @@ int compute_impl(soi_desc_t *d, const void *in, void *out, bool stage1_only)
 // With one process the all-to-all is the identity, so the round trip is
 // max_exponent per segment -> global max -> compress -> decompress, one chunk
 // per segment (chunk length l = M'/P = M').
-int run_vlc(Plan &p, void *T, cudaStream_t st)
+int run_vlc(Plan &p, const Exec &ex)
 {
   const int len = (int)(2 * p.Mh);
   if (len % 16) return SOI_ERR_UNSUPPORTED;
-  const int ns = (int)p.S;
+  cudaStream_t st = ex.st;
+  // the computed segments only (all S for a full transform)
+  void *T = (char *)ex.T + (size_t)ex.lo * p.Mh * p.elem;
+  const int ns = ex.hi - ex.lo;
   if (!p.d_vlc_words) {
+    const size_t S = p.S;
     p.vlc_stride = (long)(4 * p.Mh + 64);
-    CK(cudaMalloc(&p.d_vlc_words, (size_t)p.vlc_stride * ns * sizeof(int)));
-    CK(cudaMalloc(&p.d_vlc_n, ns * sizeof(int)));
-    CK(cudaMalloc(&p.d_vlc_emax, (ns + 1) * sizeof(int)));
-    if (p.prec != SOI_PRECISION_FP64) CK(cudaMalloc(&p.d_vlc_x, (size_t)len * ns * sizeof(double)));
+    CK(cudaMalloc(&p.d_vlc_words, (size_t)p.vlc_stride * S * sizeof(int)));
+    CK(cudaMalloc(&p.d_vlc_n, S * sizeof(int)));
+    CK(cudaMalloc(&p.d_vlc_emax, (S + 1) * sizeof(int)));
+    if (p.prec != SOI_PRECISION_FP64) CK(cudaMalloc(&p.d_vlc_x, (size_t)len * S * sizeof(double)));
   }
   double *x = p.prec == SOI_PRECISION_FP64 ? (double *)T : p.d_vlc_x;
   if (p.prec != SOI_PRECISION_FP64) {
@@ -1019,6 +948,31 @@ int soi_compute_oop_status(soi_desc_t *d, const void *in, void *out)
   return rc;
 }
 
+int soi_compute_segments_status(soi_desc_t *d, const void *in, void *out, int seg_lo, int seg_hi)
+{
+  if (!d) return SOI_ERR_INVALID;
+  int rc = (in && out) ? compute_impl(d, in, out, false, seg_lo, seg_hi) : SOI_ERR_INVALID;
+  d->last_status = rc;
+  return rc;
+}
+
+int soi_compute_async_status(soi_desc_t *d, const void *in, void *out)
+{
+  if (!d) return SOI_ERR_INVALID;
+  int rc = (in && out) ? compute_impl(d, in, out, false, 0, -1, false) : SOI_ERR_INVALID;
+  d->last_status = rc;
+  return rc;
+}
+
+int soi_check_status(soi_desc_t *d)
+{
+  Plan *p = plan_of(d);
+  if (!p) return SOI_ERR_NOT_INITIALISED;
+  if (cudaSetDevice(p->device) != cudaSuccess) return SOI_ERR_CUDA;
+  CK(cudaStreamSynchronize(p->stream));
+  return check_stage2(*p, p->d_sync, p->stream);
+}
+
 int soi_filter_subsampling_status(soi_desc_t *d, void *alpha)
 {
   if (!d) return SOI_ERR_INVALID;
@@ -1060,7 +1014,8 @@ int soi_filter_subsample_device(soi_desc_t *d, const void *alpha_dev, void *T_de
   Plan *p = plan_of(d);
   if (!p) return SOI_ERR_NOT_INITIALISED;
   if (cudaSetDevice(p->device) != cudaSuccess) return SOI_ERR_CUDA;
-  return run_stage1(*p, alpha_dev, T_dev, p->stream);
+  const Exec ex{ alpha_dev, T_dev, nullptr, p->d_sync, 0, (int)p->S, p->stream };
+  return run_stage1(*p, ex);
 }
 
 int soi_segment_fft_demod_device(soi_desc_t *d, void *T_dev, void *out_dev)
@@ -1068,8 +1023,9 @@ int soi_segment_fft_demod_device(soi_desc_t *d, void *T_dev, void *out_dev)
   Plan *p = plan_of(d);
   if (!p) return SOI_ERR_NOT_INITIALISED;
   if (cudaSetDevice(p->device) != cudaSuccess) return SOI_ERR_CUDA;
-  int rc = run_stage2(*p, T_dev, out_dev, p->stream);
-  if (rc == SOI_OK && p->fast2) rc = check_fast2(*p, p->stream);
+  const Exec ex{ nullptr, T_dev, out_dev, p->d_sync, 0, (int)p->S, p->stream };
+  int rc = run_stage2(*p, ex);
+  if (rc == SOI_OK) rc = check_stage2(*p, p->d_sync, p->stream);
   return rc;
 }
 

@@ -34,6 +34,7 @@ struct ConvArgs {
   long long Mh;          // M' rows of output
   long long J;           // M/d output groups
   int S, d, atap, JT, pitch;
+  int seg_lo, seg_hi;    // segments sigma stored (all: 0, S)
 };
 
 // Input row index (j*d + kk) mod M for the circular convolution; the ghost
@@ -149,7 +150,7 @@ __global__ void __launch_bounds__(256) k_conv_sfft(ConvArgs a)
     const int sg = idx / rows_tile;
     const int r = idx - sg * rows_tile;
     const long long rho = rho0 + r;
-    if (rho < a.Mh) T[(size_t)sg * a.Mh + rho] = tile[(size_t)r * a.pitch + permS[sg]];
+    if (rho < a.Mh && sg >= a.seg_lo && sg < a.seg_hi) T[(size_t)sg * a.Mh + rho] = tile[(size_t)r * a.pitch + permS[sg]];
   }
 }
 
@@ -166,6 +167,7 @@ struct SegArgs {
   const void *wsmall;
   long long Mh, M;
   int M1, M2, C1, C2, lo_bits;
+  int seg_lo;              // segment of blockIdx.y == 0
 };
 
 // w_{M'}^e computed in FP64 from two tables and rounded once to R.
@@ -182,7 +184,7 @@ __device__ __forceinline__ V cross_twiddle(const SegArgs &a, long long e)
   return w;
 }
 
-// Pass 1: segment blockIdx.y, columns m2 in [blockIdx.x*C1, +C1): FFT of
+// Pass 1: segment seg_lo + blockIdx.y, columns m2 in [blockIdx.x*C1, +C1): FFT of
 // length M1 over m1 of T[m1*M2 + m2], times w_{M'}^(m2*k1), stored in place
 // at k1*M2 + m2.
 template <typename R>
@@ -193,7 +195,7 @@ __global__ void __launch_bounds__(256) k_seg_cols(SegArgs a)
   V *buf = reinterpret_cast<V *>(smem_raw);
   const int C1 = a.C1, M1 = a.M1, M2 = a.M2;
   const int ps = C1 + 1;
-  V *seg = reinterpret_cast<V *>(a.T) + (size_t)blockIdx.y * a.Mh;
+  V *seg = reinterpret_cast<V *>(a.T) + (size_t)(a.seg_lo + blockIdx.y) * a.Mh;
   const int m2_0 = blockIdx.x * C1;
   const int total = M1 * C1;
   for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
@@ -212,7 +214,7 @@ __global__ void __launch_bounds__(256) k_seg_cols(SegArgs a)
   }
 }
 
-// Pass 2: segment blockIdx.y, rows k1 in [blockIdx.x*C2, +C2): FFT of length
+// Pass 2: segment seg_lo + blockIdx.y, rows k1 in [blockIdx.x*C2, +C2): FFT of length
 // M2 over m2 of row k1, giving X[k1 + M1*k2]; out[seg*M + k] = W_inv[k]*X[k]
 // for k < M (pfft.c:653-660), the other M'-M bins are dropped.
 template <typename R>
@@ -223,7 +225,7 @@ __global__ void __launch_bounds__(256) k_seg_rows_demod(SegArgs a)
   V *buf = reinterpret_cast<V *>(smem_raw);
   const int C2 = a.C2, M1 = a.M1, M2 = a.M2;
   const int ps = C2 + 1;
-  const V *seg = reinterpret_cast<const V *>(a.T) + (size_t)blockIdx.y * a.Mh;
+  const V *seg = reinterpret_cast<const V *>(a.T) + (size_t)(a.seg_lo + blockIdx.y) * a.Mh;
   const int k1_0 = blockIdx.x * C2;
   const int total = M2 * C2;
   for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
@@ -233,7 +235,7 @@ __global__ void __launch_bounds__(256) k_seg_rows_demod(SegArgs a)
   __syncthreads();
   smem_fft<V>(buf, a.plan2, C2, ps, 1, reinterpret_cast<const V *>(a.tw2),
               reinterpret_cast<const V *>(a.wsmall));
-  V *out = reinterpret_cast<V *>(a.out) + (size_t)blockIdx.y * a.M;
+  V *out = reinterpret_cast<V *>(a.out) + (size_t)(a.seg_lo + blockIdx.y) * a.M;
   const V *winv = reinterpret_cast<const V *>(a.winv);
   for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
     const int k2 = idx / C2, c = idx - k2 * C2;

@@ -28,6 +28,7 @@ struct Conv2Args {
   long long M, Mh, J;
   int S, d, atap, JT, pitch, AC;
   int buf_elems;         // complex elements per staging buffer (rows + filter, rounded)
+  int seg_lo, seg_hi;    // segments sigma stored (all: 0, S)
 };
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
@@ -176,7 +177,7 @@ __global__ void __launch_bounds__(512, 1) k_conv_sfft_staged(Conv2Args a)
     const int sg = idx / rows_tile;
     const int r = idx - sg * rows_tile;
     const long long rho = rho0 + r;
-    if (rho < a.Mh) T[(size_t)sg * a.Mh + rho] = tile[(size_t)r * a.pitch + permS[sg]];
+    if (rho < a.Mh && sg >= a.seg_lo && sg < a.seg_hi) T[(size_t)sg * a.Mh + rho] = tile[(size_t)r * a.pitch + permS[sg]];
   }
 }
 
@@ -185,13 +186,16 @@ __global__ void __launch_bounds__(512, 1) k_conv_sfft_staged(Conv2Args a)
 // store of .cpp:391 / the all-to-all of pfft.c:554-578), consecutive threads
 // on consecutive rows rho.
 template <typename V> struct EmitTransposed {
-  V *T; long long Mh, rho0;
+  V *T; long long Mh, rho0; int lo, hi;   // segments f in [lo, hi) are stored
   template <int RL> __device__ __forceinline__ void run(int col, int fbase, int fstep, V *v) const
   {
     const long long rho = rho0 + col;
     if (rho < Mh) {
 #pragma unroll
-      for (int k = 0; k < RL; ++k) T[(size_t)(fbase + fstep * k) * Mh + rho] = v[k];
+      for (int k = 0; k < RL; ++k) {
+        const int f = fbase + fstep * k;
+        if (f >= lo && f < hi) T[(size_t)f * Mh + rho] = v[k];
+      }
     }
   }
 };
@@ -320,7 +324,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_conv_sfft_tS(Conv2Args a)
     }
   }
   __syncthreads();
-  EmitTransposed<V> e{ reinterpret_cast<V *>(a.T), a.Mh, (long long)NMU * j0 };
+  EmitTransposed<V> e{ reinterpret_cast<V *>(a.T), a.Mh, (long long)NMU * j0, a.seg_lo, a.seg_hi };
   tile_fft_smem<V, R0, R1, 1>(tile, rows_tile, 1, PITCH, twS, e);
 }
 

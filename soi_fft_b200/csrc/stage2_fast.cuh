@@ -1,50 +1,52 @@
 // stage2_fast.cuh -- the M'-point FFT of every segment with the demodulation
-// epilogue (pfft.c:642,649-694), as one persistent kernel.
+// epilogue (pfft.c:642,649-694), as one persistent kernel with the tile
+// geometry fixed at compile time.
 //
-// Four-step split M' = M1*M2.  Pass 1 of segment s (tile = C1 columns m2):
+// Four-step split M' = M1*M2.  Pass 1 of segment s (tile = C columns m2):
 // FFT of length M1 over m1 of T[s][m1*M2 + m2], times w_{M'}^(m2*k1), written
-// in place.  Pass 2 (tile = C2 rows k1): FFT of length M2 of row k1, output
-// k = k1 + M1*k2, times W_inv[k], stored for k < M.
+// in place.  Pass 2 (tile = C rows k1): FFT of length M2 of row k1, output
+// k = k1 + M1*k2, times W_inv[k], stored for k < M (the discard).
 //
 // Each tile FFT is an in-place decimation-in-frequency transform with "fat"
-// radices held in registers (RegDFT): the first radix stage loads straight
-// from HBM and the last stores straight to HBM, so a tile makes one (two for a
-// three-stage split) round trip through shared memory.
+// radices held in registers (RegDFT), two or three radix stages with one pass
+// through shared memory between stages; the last stage stores straight to
+// global memory through the epilogue.
+//
+// C = 32 bytes / element size: every strided row run of a tile (pass-1 loads
+// and stores, pass-2 output stores) is one full 32-byte sector, so each L2
+// request moves a whole sector.
+//
+// Epilogue factors come from per-task tables instead of scattered lookups.
+// Pass 1: w_{M'}^(m2*f) for f = fbase + fstep*k is base(m2*fbase) times
+// step[col][k] = w_{M'}^(m2*fstep*k), the C x RL step table built per task in
+// shared memory.  Pass 2: W_inv[k], k = k1 + M1*k2, is
+// amp[min(k, M-k)] * ph(k1) * ph(M1*k2) with ph(k) = exp(-i pi kappa k/M);
+// ph(k1) per task in shared memory, ph(M1*k2) from an M2-entry table.  Every
+// table entry is FP64-generated and rounded once; the products are formed in
+// the working precision.
 //
 // Schedule: CTAs take tasks from a global counter in the order
 //   P1(0), P1(1), P2(0), P1(2), P2(1), ..., P2(S-1),
 // so that only two segments' intermediates (2 * M' * 8 bytes, 84 MB at
-// N = 2^29) are live; they stay in L2 between the passes.  A pass-2 task of
-// segment s waits, with an iteration limit, until all pass-1 tasks of s have
-// published their tiles (per-segment counter, release/acquire at gpu scope).
-// Pass-2 tasks then drop the lines they consumed from L2 without write-back
-// (discard.global.L2), so the dead intermediate never returns to HBM.
+// N = 2^29 in FP32) are live; they stay in L2 between the passes.  A pass-2
+// task of segment s waits, with an iteration limit, until all pass-1 tasks of
+// s have published their tiles (per-segment counter, release/acquire at gpu
+// scope).  Pass-2 tasks then drop the lines they consumed from L2 without
+// write-back (discard.global.L2), so the dead intermediate never returns to
+// HBM.  The CTA claims its next task while it works on the current one.  A
+// CTA holds at most one claimed task it has not started, and a pass-2 task
+// only waits on tasks with smaller indices, so the lowest unfinished task can
+// always run.  A wait that gives up sets the error flag, and every CTA then
+// stops taking tasks; the host reads the flag (SOI_ERR_TIMEOUT).
+//
+// The kernel works on the segment range [seg_lo, seg_lo + S) of the buffers
+// (all segments for a full transform, a band of segments for a
+// segments-of-interest transform).
 #pragma once
 
 #include "fft_reg.cuh"
 
 namespace soi {
-
-struct S2Args {
-  void *T;                    // [S][Mh], pass-1 input, intermediate in place
-  void *out;                  // [S][M]
-  const void *tw1;            // exp(-2 pi i m/M1), m < M1
-  const void *tw2;            // exp(-2 pi i m/M2)
-  const double2 *xlo, *xhi;   // cross twiddles, FP64 two-level
-  const void *winv;           // [M] (unused by the persistent kernel)
-  const void *amp;            // [M/2 + 1] real: 1 / y_W(k/M - 1/2)
-  const double2 *dlo, *dhi;   // exp(-i pi kappa k / M), FP64 two-level
-  int dlo_bits;
-  int buf_elems;              // complex elements per tile buffer
-  long long Mh, M;
-  int M1, M2, C1, C2, S, lo_bits;
-  int nt1, nt2;               // tasks per segment (M2/C1, M1/C2)
-  int ps2;                    // column stride of the pass-2 tile (elements)
-  int discard;                // drop consumed intermediate lines from L2
-  unsigned int *counter;      // [1] task counter, zero before launch
-  unsigned int *done1;        // [S] pass-1 tasks finished per segment, zero before launch
-  int *err;                   // [1] set to 1 when a wait gives up
-};
 
 constexpr long long kWaitLimit = 1ll << 22;   // ~1 s of 256 ns sleeps
 
@@ -60,23 +62,9 @@ __device__ __forceinline__ void discard_l2_line(const void *p)
   asm volatile("discard.global.L2 [%0], 128;" ::"l"(p) : "memory");
 }
 
-template <typename V> __device__ __forceinline__ V ldcg(const V *p);
-template <> __device__ __forceinline__ float2 ldcg<float2>(const float2 *p) { return __ldcg(p); }
-template <> __device__ __forceinline__ double2 ldcg<double2>(const double2 *p) { return __ldcg(p); }
 template <typename V> __device__ __forceinline__ void stcs(V *p, V v);
 template <> __device__ __forceinline__ void stcs<float2>(float2 *p, float2 v) { __stcs(p, v); }
 template <> __device__ __forceinline__ void stcs<double2>(double2 *p, double2 v) { __stcs(p, v); }
-
-template <typename V>
-__device__ __forceinline__ V cross_tw(const S2Args &a, long long e)
-{
-  const double2 lo = __ldg(a.xlo + (e & ((1ll << a.lo_bits) - 1)));
-  const double2 hi = __ldg(a.xhi + (e >> a.lo_bits));
-  V w;
-  w.x = (decltype(w.x))(hi.x * lo.x - hi.y * lo.y);
-  w.y = (decltype(w.y))(hi.x * lo.y + hi.y * lo.x);
-  return w;
-}
 
 __device__ __forceinline__ void cp_async_8(void *smem, const void *gmem)
 {
@@ -90,174 +78,6 @@ __device__ __forceinline__ void cp_async_16cg(void *smem, const void *gmem)
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-__device__ __forceinline__ void cp_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
-
-// e^{-i pi kappa k / M} in FP64 from two tables, then times the real
-// amplitude 1/y_W (pfft.c:68-82 factorised; amp is symmetric, amp[k] =
-// amp[M-k], stored for k <= M/2)
-template <typename V>
-__device__ __forceinline__ V demod_factor(const S2Args &a, long long k)
-{
-  const double2 lo = __ldg(a.dlo + (k & ((1ll << a.dlo_bits) - 1)));
-  const double2 hi = __ldg(a.dhi + (k >> a.dlo_bits));
-  const long long km = k <= a.M / 2 ? k : a.M - k;
-  const double amp = (double)__ldg(reinterpret_cast<const decltype(V::x) *>(a.amp) + km);
-  V w;
-  w.x = (decltype(w.x))((hi.x * lo.x - hi.y * lo.y) * amp);
-  w.y = (decltype(w.y))((hi.x * lo.y + hi.y * lo.x) * amp);
-  return w;
-}
-
-template <typename V> struct EmitCols {
-  const S2Args *a; V *Tseg; int m2_0;
-  template <int RL> __device__ __forceinline__ void run(int col, int fbase, int fstep, V *v) const
-  {
-    constexpr int CH = RL < 8 ? RL : 8;
-#pragma unroll
-    for (int c0 = 0; c0 < RL; c0 += CH) {
-      V w[CH];
-#pragma unroll
-      for (int k = 0; k < CH; ++k) w[k] = cross_tw<V>(*a, (long long)(m2_0 + col) * (fbase + fstep * (c0 + k)));
-#pragma unroll
-      for (int k = 0; k < CH; ++k)
-        Tseg[(size_t)(fbase + fstep * (c0 + k)) * a->M2 + m2_0 + col] = cmul(v[c0 + k], w[k]);
-    }
-  }
-};
-
-template <typename V> struct EmitRows {
-  const S2Args *a; V *out; int k1_0;
-  template <int RL> __device__ __forceinline__ void run(int col, int fbase, int fstep, V *v) const
-  {
-    constexpr int CH = RL < 8 ? RL : 8;
-#pragma unroll
-    for (int c0 = 0; c0 < RL; c0 += CH) {
-      V w[CH];
-      long long kk[CH];
-#pragma unroll
-      for (int k = 0; k < CH; ++k) {
-        kk[k] = (long long)(k1_0 + col) + (long long)a->M1 * (fbase + fstep * (c0 + k));
-        w[k] = kk[k] < a->M ? demod_factor<V>(*a, kk[k]) : v[c0 + k];
-      }
-#pragma unroll
-      for (int k = 0; k < CH; ++k)
-        if (kk[k] < a->M) stcs(out + kk[k], cmul(w[k], v[c0 + k]));
-    }
-  }
-};
-
-template <typename R, int A0, int A1, int A2, int B0, int B1, int B2>
-__global__ void __launch_bounds__(128, 4) k_stage2_persistent(S2Args a)
-{
-  using V = typename cplx_of<R>::type;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  V *buf = reinterpret_cast<V *>(smem_raw);
-  __shared__ unsigned int s_task;
-  __shared__ int s_ok;
-  constexpr int RLA = A2 > 1 ? A2 : A1;
-  constexpr int RLB = B2 > 1 ? B2 : B1;
-  const unsigned int per = (unsigned int)(a.nt1 + a.nt2);
-  const unsigned int total = (unsigned int)a.S * per;
-
-  for (;;) {
-    // claim a task; a pass-2 task waits (bounded) for its segment's pass 1.
-    // The CTA holds no other unfinished task while it waits.
-    if (threadIdx.x == 0) {
-      unsigned int t = atomicAdd(a.counter, 1u);
-      if (*(volatile int *)a.err) t = total;
-      int ok = 1;
-      if (t < total) {
-        if (t >= (unsigned int)a.nt1) {
-          const unsigned int u = t - a.nt1;
-          const int blk = (int)(u / per), r = (int)(u % per);
-          const bool p2 = blk >= a.S - 1 || r >= a.nt1;
-          if (p2) {
-            long long it = 0;
-            while (ld_acquire_u32(a.done1 + blk) < (unsigned int)a.nt1) {
-              if (++it > kWaitLimit) { atomicExch(a.err, 1); ok = 0; break; }
-              __nanosleep(128);
-            }
-          }
-        }
-      }
-      s_task = t;
-      s_ok = ok;
-    }
-    __syncthreads();
-    const unsigned int t = s_task;
-    const int ok = s_ok;
-    __syncthreads();
-    if (t >= total || !ok) break;
-    int kind, seg, tile;
-    if (t < (unsigned int)a.nt1) { kind = 1; seg = 0; tile = (int)t; }
-    else {
-      const unsigned int u = t - a.nt1;
-      const int blk = (int)(u / per), r = (int)(u % per);
-      if (blk < a.S - 1) {
-        if (r < a.nt1) { kind = 1; seg = blk + 1; tile = r; }
-        else { kind = 2; seg = blk; tile = r - a.nt1; }
-      } else { kind = 2; seg = a.S - 1; tile = r; }
-    }
-    V *Tseg = reinterpret_cast<V *>(a.T) + (size_t)seg * a.Mh;
-    if (kind == 1) {
-      // C1 = 2 columns: one 16-byte copy per row
-      const int m2_0 = tile * a.C1;
-      for (int pos = threadIdx.x; pos < a.M1; pos += blockDim.x)
-        cp_async_16cg(buf + (size_t)(pos + pos / RLA) * a.C1, Tseg + (size_t)pos * a.M2 + m2_0);
-      cp_commit();
-      cp_wait_all();
-      __syncthreads();
-      EmitCols<V> e{ &a, Tseg, m2_0 };
-      tile_fft_smem<V, A0, A1, A2>(buf, a.C1, a.C1, 1, reinterpret_cast<const V *>(a.tw1), e);
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        __threadfence();
-        atomicAdd(a.done1 + seg, 1u);
-      }
-    } else {
-      const int k1_0 = tile * a.C2;
-      const int n = a.C2 * a.M2;
-      for (int q = threadIdx.x; q < n; q += blockDim.x) {
-        const int col = q / a.M2, pos = q - col * a.M2;
-        cp_async_8(buf + (size_t)(pos + pos / RLB) + (size_t)col * a.ps2, Tseg + (size_t)(k1_0 + col) * a.M2 + pos);
-      }
-      cp_commit();
-      cp_wait_all();
-      __syncthreads();
-      if (a.discard) {
-        // the tile's rows are in shared memory now; their L2 lines are dead
-        const char *base = reinterpret_cast<const char *>(Tseg + (size_t)k1_0 * a.M2);
-        const long long nlines = ((long long)a.C2 * a.M2 * sizeof(V)) / 128;
-        for (long long l = threadIdx.x; l < nlines; l += blockDim.x) discard_l2_line(base + l * 128);
-      }
-      EmitRows<V> e{ &a, reinterpret_cast<V *>(a.out) + (size_t)seg * a.M, k1_0 };
-      tile_fft_smem<V, B0, B1, B2>(buf, a.C2, 1, a.ps2, reinterpret_cast<const V *>(a.tw2), e);
-    }
-    __syncthreads();
-  }
-}
-
-
-// ---------------------------------------------------------------------------
-// Stage 2 with the tile geometry fixed at compile time.
-//
-// Tasks and schedule as in k_stage2_persistent.  Differences:
-//  * C1 = C2 = 32 bytes / element size: every strided row run of a tile
-//    (pass-1 loads and stores, pass-2 output stores) is one full 32-byte
-//    sector, so each L2 request moves a whole sector.
-//  * Epilogue factors come from per-task tables instead of scattered lookups.
-//    Pass 1: w_{M'}^(m2*f) for f = fbase + fstep*k is base(m2*fbase) times
-//    step[col][k] = w_{M'}^(m2*fstep*k), the C1 x RL step table built per
-//    task in shared memory.  Pass 2: W_inv[k], k = k1 + M1*k2, is
-//    amp[min(k, M-k)] * ph(k1) * ph(M1*k2) with ph(k) = exp(-i pi kappa k/M);
-//    ph(k1) per task in shared memory, ph(M1*k2) from an M2-entry table.
-//    Every table entry is FP64-generated and rounded once; the products are
-//    formed in the working precision.
-//  * The CTA claims its next task while it works on the current one.  A CTA
-//    holds at most one claimed task it has not started, and a pass-2 task only
-//    waits on tasks with smaller indices, so the lowest unfinished task can
-//    always run.
-// ---------------------------------------------------------------------------
 
 struct S2ArgsCT {
   void *T;                    // [S][Mh] pass-1 input, intermediate in place
@@ -268,7 +88,9 @@ struct S2ArgsCT {
   const double2 *dlo, *dhi;   // exp(-i pi kappa k/M) two-level, FP64
   const void *ph2;            // [M2] complex: exp(-i pi kappa M1 k2 / M)
   int lo_bits, dlo_bits;
-  int M, S;
+  int M;
+  int S;                      // segments in this launch
+  int seg_lo;                 // first segment of this launch
   int discard;
   unsigned int *counter, *done1;
   int *err;
@@ -391,7 +213,7 @@ __global__ void __launch_bounds__(NT, 2) k_stage2_ct(S2ArgsCT a)
       if (blk < a.S - 1 && r < G::NT1) { kind = 1; seg = blk + 1; tile = r; }
       else { kind = 2; seg = blk; tile = r - (blk < a.S - 1 ? G::NT1 : 0); }
     }
-    V *Tseg = reinterpret_cast<V *>(a.T) + (size_t)seg * ((size_t)M1 * M2);
+    V *Tseg = reinterpret_cast<V *>(a.T) + (size_t)(a.seg_lo + seg) * ((size_t)M1 * M2);
     if (kind == 1) {
       const int m2_0 = tile * C;
       // rows m1 of C columns: 32 bytes = 2 chunks of 16
@@ -438,7 +260,7 @@ __global__ void __launch_bounds__(NT, 2) k_stage2_ct(S2ArgsCT a)
         constexpr int nlines = C * M2 * G::E / 128;
         for (int l = tid; l < nlines; l += NT) discard_l2_line(base + l * 128);
       }
-      EmitRowsCT<V, M1, RLB> e{ reinterpret_cast<V *>(a.out) + (size_t)seg * a.M, k1_0, s_tab, &a };
+      EmitRowsCT<V, M1, RLB> e{ reinterpret_cast<V *>(a.out) + (size_t)(a.seg_lo + seg) * a.M, k1_0, s_tab, &a };
       tile_fft_ct<V, B0, B1, B2, C, 1, G::PS2, NT>(buf, reinterpret_cast<const V *>(a.tw2), e);
     }
     __syncthreads();

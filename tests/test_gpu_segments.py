@@ -1,0 +1,126 @@
+"""Segments of interest (soi_compute_segments_status), the non-waiting compute
+(soi_compute_async_status + soi_check_status) and its capture into a CUDA
+graph.  The segment outputs must be bit-identical to the same segments of a
+full compute (same kernels, same arithmetic), and nothing outside the band
+may be written."""
+import numpy as np
+import pytest
+
+import soi_fft_b200 as sb
+from tests import signals
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+# (N, S, precision): the two-kernel stage 2 (small M'), and the persistent
+# stage 2 in both precisions (M' = 320 x 256 and 320 x 512)
+SHAPES = [
+    (1 << 16, 8, sb.PRECISION_FP64),
+    (1 << 20, 16, sb.PRECISION_SPLIT_FP32),
+    (1 << 20, 8, sb.PRECISION_FP64),
+    (1 << 22, 32, sb.PRECISION_SPLIT_FP32),
+]
+
+
+def _input(N, prec, seed=7):
+    x = signals.gaussian(N, seed)
+    if prec == sb.PRECISION_SPLIT_FP32:
+        x = x.astype(np.complex64)
+    return torch.from_numpy(x).cuda()
+
+
+def _desc(N, S, prec, **kw):
+    return sb.SoiDescriptor(N=N, precision=prec, **kw).init(S)
+
+
+@pytest.mark.parametrize("N,S,prec", SHAPES)
+@pytest.mark.parametrize("band", [(0, 1), (3, 5), "last", "all"])
+def test_segments_are_bit_identical_to_full_compute(N, S, prec, band):
+    x = _input(N, prec)
+    d = _desc(N, S, prec)
+    try:
+        full = torch.empty_like(x)
+        d.compute_into(x, full)
+        lo, hi = (S - 2, S) if band == "last" else (0, S) if band == "all" else band
+        M = N // S
+        sentinel = torch.full_like(x, complex(1234.5, -77.25))
+        part = sentinel.clone()
+        d.compute_segments(x, part, lo, hi)
+        torch.cuda.synchronize()
+        assert torch.equal(part[lo * M:hi * M], full[lo * M:hi * M])
+        assert torch.equal(part[:lo * M], sentinel[:lo * M])
+        assert torch.equal(part[hi * M:], sentinel[hi * M:])
+        # a full compute after a band compute is unaffected by the band's state
+        again = torch.empty_like(x)
+        d.compute_into(x, again)
+        assert torch.equal(again, full)
+    finally:
+        d.free()
+
+
+def test_segments_with_host_buffers():
+    N, S, prec = 1 << 18, 16, sb.PRECISION_SPLIT_FP32
+    x = signals.gaussian(N, 3).astype(np.complex64)
+    d = _desc(N, S, prec)
+    try:
+        full = np.empty_like(x)
+        d.compute_into(x, full)
+        part = np.zeros_like(x)
+        d.compute_segments(x, part, 5, 9)
+        M = N // S
+        assert np.array_equal(part[5 * M:9 * M], full[5 * M:9 * M])
+        assert not part[:5 * M].any() and not part[9 * M:].any()
+    finally:
+        d.free()
+
+
+def test_segment_range_is_checked():
+    N, S, prec = 1 << 16, 8, sb.PRECISION_FP64
+    x = _input(N, prec)
+    d = _desc(N, S, prec)
+    try:
+        y = torch.empty_like(x)
+        for lo, hi in [(-1, 2), (3, 3), (5, 4), (0, S + 1)]:
+            with pytest.raises(sb.SoiError):
+                d.compute_segments(x, y, lo, hi)
+    finally:
+        d.free()
+
+
+@pytest.mark.parametrize("N,S,prec", SHAPES)
+def test_async_compute_matches_and_checks(N, S, prec):
+    x = _input(N, prec)
+    d = _desc(N, S, prec)
+    try:
+        ref = torch.empty_like(x)
+        d.compute_into(x, ref)
+        y = torch.empty_like(x)
+        d.compute_async(x, y)
+        d.check()
+        assert torch.equal(y, ref)
+    finally:
+        d.free()
+
+
+@pytest.mark.parametrize("N,S,prec", [(1 << 20, 16, sb.PRECISION_SPLIT_FP32), (1 << 20, 8, sb.PRECISION_FP64)])
+def test_async_compute_captures_into_a_cuda_graph(N, S, prec):
+    s = torch.cuda.Stream()
+    x = _input(N, prec)
+    d = _desc(N, S, prec, stream=s.cuda_stream)
+    try:
+        ref = torch.empty_like(x)
+        d.compute_into(x, ref)
+        torch.cuda.synchronize()
+        y = torch.zeros_like(x)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s):
+            d.compute_async(x, y)
+        for _ in range(3):
+            y.zero_()
+            g.replay()
+            torch.cuda.synchronize()
+            d.check()
+            assert torch.equal(y, ref)
+        del g
+    finally:
+        d.free()

@@ -151,6 +151,38 @@ int soi_set_timing(soi_desc_t *desc, int enable);
  * soi_status_t error.  No counterpart in the reference (no GPU there). */
 int soi_kernels_per_compute(soi_desc_t *desc);
 
+/* ---- batched transforms ------------------------------------------------ */
+/* No counterpart in the reference, which transforms one signal per call.
+ * A batch is a fixed set of transforms on device buffers, replayed as one
+ * CUDA graph: one plan per distinct (N, k) (with `tune`, the fastest of the
+ * plan's kernel variants, timed once on the first transform of that shape),
+ * the transforms spread over `chains` concurrent streams (each with its own
+ * scratch, in order within a chain).  Window, oversampling, precision,
+ * device and use_vlc come from `tmpl` (a descriptor set up as for
+ * init_soi_descriptor; its N is ignored).  With use_vlc the batch runs one
+ * chain. */
+typedef struct soi_batch soi_batch_t;
+typedef struct {
+  cfft_size_t N;          /* transform length                                  */
+  cfft_size_t k;          /* segments (the reference's k with P = 1)           */
+  int seg_lo, seg_hi;     /* segments of interest; seg_hi <= 0: all k           */
+  const void *in;         /* device input, N complex (complex64 in split form)  */
+  void *out;              /* device output, N complex; may equal in            */
+} soi_batch_item_t;
+int soi_batch_create(soi_batch_t **batch, const soi_desc_t *tmpl, const soi_batch_item_t *items, int count,
+                     int chains, int tune);
+/* Launches the batch's graph on `stream` (a cudaStream_t; NULL = legacy). */
+int soi_batch_execute(soi_batch_t *batch, void *stream);
+/* Waits for the last execute; SOI_ERR_TIMEOUT if a stage-2 wait gave up. */
+int soi_batch_check(soi_batch_t *batch);
+/* info[0..7] = transforms, plans, chains, graph nodes, kernel launches per
+ * execute, scratch bytes, 0, 0. */
+int soi_batch_info(soi_batch_t *batch, long long *info);
+/* Plan `plan`: info[0..7] = N, k, stage-1 block size, persistent stage 2
+ * (1/0), M1, M2, tuned time (microseconds, 0 untuned), variant code. */
+int soi_batch_plan_info(soi_batch_t *batch, int plan, long long *info);
+int soi_batch_destroy(soi_batch_t *batch);
+
 /* ---- VLC (compress.c) on the device ------------------------------------ */
 
 /* compress.c:11-131 over nchunks chunks of `len` doubles each (device

@@ -60,13 +60,16 @@ struct Plan {
   int dlo_bits = 11;
   void (*f2ct_kernel)(S2ArgsCT) = nullptr;
   void *d_ph2 = nullptr;            // [M2] complex exp(-i pi kappa M1 k2 / M)
-  unsigned int *d_sync = nullptr;   // [0] counter, [1] err, [2..2+S) done1
+  unsigned int *d_sync = nullptr;   // [0] err, [1] counter, [2..2+S) done1
   // staged stage 1
   int s1fast = 0, JR2 = 0, JT2 = 0, AC = 0, buf_elems = 0;
   int s1_tS = 0;                    // compile-time-S stage-1 instance available
   int s1_nt = 512;                  // its block size (256: two CTAs per SM)
   size_t smem1b = 0;
   void *d_filt2 = nullptr;          // [d][atap][nmu][S] real
+  // variant choices forced by the batch tuner (-1: defaults / SOI_* switches)
+  int knob_s1_nt = -1;              // 256 or 512 threads for the compile-time-S stage 1
+  int knob_s2 = -1;                 // 1 persistent stage 2, 0 two-kernel stage 2
   bool timing = false;
   cudaEvent_t ev[5] = {};
   float ms[4] = {0, 0, 0, 0};
@@ -80,7 +83,7 @@ struct Exec {
   const void *in;              // N inputs [M rows][S]
   void *T;                     // S x M' transposed data
   void *out;                   // N outputs [S][M] (rows of segments outside [lo, hi) untouched)
-  unsigned int *sync;          // [0] task counter, [1] error flag, [2 .. 2 + S) pass-1 counts
+  unsigned int *sync;          // [0] error flag (sticky), [1] task counter, [2 .. 2 + S) pass-1 counts
   int lo, hi;                  // segments computed
   cudaStream_t st;
 };
@@ -333,8 +336,8 @@ const S2ChoiceCT kS2CT[] = {
 // index into kS2CT for M' and the element size, or -1
 int pick_s2ct(const Plan &p)
 {
-  // SOI_STAGE2_FAST=0 selects the two-kernel path
-  if (env_int("SOI_STAGE2_FAST", 1) == 0) return -1;
+  // SOI_STAGE2_FAST=0 (or the tuner) selects the two-kernel path
+  if (p.knob_s2 == 0 || (p.knob_s2 < 0 && env_int("SOI_STAGE2_FAST", 1) == 0)) return -1;
   for (int i = 0; i < (int)(sizeof(kS2CT) / sizeof(kS2CT[0])); ++i)
     if ((long long)kS2CT[i].M1 * kS2CT[i].M2 == (long long)p.Mh && kS2CT[i].elem == (int)p.elem) return i;
   return -1;
@@ -411,8 +414,9 @@ int launch_s2ct(Plan &p, const Exec &ex)
   a.lo_bits = p.lo_bits; a.dlo_bits = p.dlo_bits; a.M = (int)p.M;
   a.S = ex.hi - ex.lo; a.seg_lo = ex.lo;
   a.discard = p.discard;
-  a.counter = ex.sync; a.err = (int *)(ex.sync + 1); a.done1 = ex.sync + 2;
-  CK(cudaMemsetAsync(ex.sync, 0, (size_t)(a.S + 2) * sizeof(unsigned int), ex.st));
+  a.err = (int *)ex.sync; a.counter = ex.sync + 1; a.done1 = ex.sync + 2;
+  // counters restart; the error flag stays set until the owner clears it
+  CK(cudaMemsetAsync(ex.sync + 1, 0, (size_t)(a.S + 1) * sizeof(unsigned int), ex.st));
   p.f2ct_kernel<<<p.f2_grid, 256, p.f2_smem, ex.st>>>(a);
   CK(cudaGetLastError());
   return SOI_OK;
@@ -424,7 +428,7 @@ int check_stage2(Plan &p, const unsigned int *sync, cudaStream_t st)
 {
   if (!p.fast2 || !sync) return SOI_OK;
   int err = 0;
-  CK(cudaMemcpyAsync(&err, sync + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(&err, sync, sizeof(int), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   return err ? SOI_ERR_TIMEOUT : SOI_OK;
 }
@@ -534,7 +538,8 @@ void plan_stage1_staged(Plan &p)
   // compile-time-S kernel: 256 threads and <= 110 KB (two CTAs per SM) where
   // a tile of at least two thread rows fits, else 512 threads and 200 KB
   int nt = 512;
-  if (ts && 2 * (int)p.S <= 256) nt = env_int("SOI_STAGE1_NT", 256) == 512 ? 512 : 256;
+  if (ts && 2 * (int)p.S <= 256)
+    nt = (p.knob_s1_nt > 0 ? p.knob_s1_nt : env_int("SOI_STAGE1_NT", 256)) == 512 ? 512 : 256;
   const int groups = nt / (int)p.S;
   const size_t budget = (nt == 256 ? 110 * 1024 : 200 * 1024) - p.S * (p.elem + sizeof(int));
   const size_t real = p.elem / 2;
@@ -736,9 +741,14 @@ int plan_geometry(const soi_desc_t *d, size_t k, Plan &p)
   return choose_split(p);
 }
 
-int init_plan(soi_desc_t *d, size_t k)
+// A device plan for k segments of d's transform.  with_stream: the plan gets
+// the descriptor's stream (or its own) and timing events, as a descriptor's
+// plan; the batch driver's plans run on the batch's streams instead.
+int make_plan(const soi_desc_t *d, size_t k, int knob_s1_nt, int knob_s2, bool with_stream, Plan **out)
 {
   Plan *p = new Plan();
+  p->knob_s1_nt = knob_s1_nt;
+  p->knob_s2 = knob_s2;
   int rc = plan_geometry(d, k, *p);
   if (rc) { delete p; return rc; }
   cudaError_t ce = cudaSetDevice(d->device);
@@ -750,6 +760,10 @@ int init_plan(soi_desc_t *d, size_t k)
     p->fast2 = 0;
     if ((rc = setup_s2ct(*p, p->f2_variant))) { free_plan(p); return rc; }
   }
+  if (!with_stream) {
+    *out = p;
+    return SOI_OK;
+  }
   if (cudaMalloc(&p->d_T, p->S * p->Mh * p->elem) != cudaSuccess) { free_plan(p); return SOI_ERR_CUDA; }
   if (d->stream) {
     p->stream = (cudaStream_t)d->stream;
@@ -759,15 +773,24 @@ int init_plan(soi_desc_t *d, size_t k)
   }
   for (auto &e : p->ev)
     if (cudaEventCreate(&e) != cudaSuccess) { free_plan(p); return SOI_ERR_CUDA; }
+  *out = p;
+  return SOI_OK;
+}
+
+int init_plan(soi_desc_t *d, size_t k)
+{
+  Plan *p = nullptr;
+  int rc = make_plan(d, k, -1, -1, true, &p);
+  if (rc) return rc;
   d->plan = p;
   return SOI_OK;
 }
 
 Plan *plan_of(soi_desc_t *d) { return d ? (Plan *)d->plan : nullptr; }
 
-// One transform: in -> out (they may alias, the reference's in-place form).
-// Host pointers are staged through the plan's device buffer.
-// The transform of `in` into `out` for segments [seg_lo, seg_hi).  With
+// One transform: in -> out (they may alias, the reference's in-place form),
+// for segments [seg_lo, seg_hi).  Host pointers are staged through the
+// plan's device buffer.  With
 // sync_after false the work is only enqueued (nothing waits on the stream,
 // so it can be captured into a CUDA graph); soi_check_status reads the
 // stage-2 error flag afterwards.
@@ -792,6 +815,7 @@ int compute_impl(soi_desc_t *d, const void *in, void *out, bool stage1_only, int
   }
   int rc;
   const Exec ex{ src, p->d_T, dst, p->d_sync, seg_lo, seg_hi, st };
+  if (p->fast2) CK(cudaMemsetAsync(p->d_sync, 0, sizeof(unsigned int), st));   // error flag
   if (p->timing) CK(cudaEventRecord(p->ev[0], st));
   if ((rc = run_stage1(*p, ex))) return rc;
   if (p->timing) CK(cudaEventRecord(p->ev[1], st));
@@ -826,6 +850,20 @@ int compute_impl(soi_desc_t *d, const void *in, void *out, bool stage1_only, int
 // With one process the all-to-all is the identity, so the round trip is
 // max_exponent per segment -> global max -> compress -> decompress, one chunk
 // per segment (chunk length l = M'/P = M').
+// VLC buffers of a plan (words, counts, exponents; the promoted copy in the
+// split form), allocated once
+int vlc_alloc(Plan &p)
+{
+  if (p.d_vlc_words) return SOI_OK;
+  const size_t S = p.S, len = 2 * p.Mh;
+  p.vlc_stride = (long)(4 * p.Mh + 64);
+  CK(cudaMalloc(&p.d_vlc_words, (size_t)p.vlc_stride * S * sizeof(int)));
+  CK(cudaMalloc(&p.d_vlc_n, S * sizeof(int)));
+  CK(cudaMalloc(&p.d_vlc_emax, (S + 1) * sizeof(int)));
+  if (p.prec != SOI_PRECISION_FP64) CK(cudaMalloc(&p.d_vlc_x, len * S * sizeof(double)));
+  return SOI_OK;
+}
+
 int run_vlc(Plan &p, const Exec &ex)
 {
   const int len = (int)(2 * p.Mh);
@@ -834,14 +872,8 @@ int run_vlc(Plan &p, const Exec &ex)
   // the computed segments only (all S for a full transform)
   void *T = (char *)ex.T + (size_t)ex.lo * p.Mh * p.elem;
   const int ns = ex.hi - ex.lo;
-  if (!p.d_vlc_words) {
-    const size_t S = p.S;
-    p.vlc_stride = (long)(4 * p.Mh + 64);
-    CK(cudaMalloc(&p.d_vlc_words, (size_t)p.vlc_stride * S * sizeof(int)));
-    CK(cudaMalloc(&p.d_vlc_n, S * sizeof(int)));
-    CK(cudaMalloc(&p.d_vlc_emax, (S + 1) * sizeof(int)));
-    if (p.prec != SOI_PRECISION_FP64) CK(cudaMalloc(&p.d_vlc_x, (size_t)len * S * sizeof(double)));
-  }
+  int rc;
+  if ((rc = vlc_alloc(p))) return rc;
   double *x = p.prec == SOI_PRECISION_FP64 ? (double *)T : p.d_vlc_x;
   if (p.prec != SOI_PRECISION_FP64) {
     vlc_promote<<<1024, 256, 0, st>>>((const float *)T, x, (long long)len * ns);
@@ -870,6 +902,242 @@ void die_on(int rc, const char *what)
   if (rc == SOI_OK) return;
   fprintf(stderr, "%s: %s\n", what, soi_status_string(rc));
   exit(-1);
+}
+
+// ---- batch driver ---------------------------------------------------------------
+//
+// Many independent transforms (of different lengths, segment counts and
+// segment bands) as one CUDA graph.  One plan per distinct (N, k), shared by
+// all transforms of that shape; with tuning, the plan is the fastest of its
+// variants (stage-1 block size, persistent or two-kernel stage 2) timed on
+// the first transform of that shape.  The transforms are spread over
+// `chains` streams by estimated work (largest first onto the least-loaded
+// chain); each chain has its own transposed-data scratch and stage-2
+// synchronisation words, so chains run concurrently and the transforms of a
+// chain run in order.  The graph forks the chains from the launch stream and
+// joins them back.
+
+struct BatchItem {
+  size_t N, k;
+  int lo, hi;
+  const void *in;
+  void *out;
+  int plan = -1, chain = -1;
+  double work = 0;
+};
+
+struct Batch {
+  int device = 0;
+  soi_desc_t tmpl{};
+  std::vector<Plan *> plans;
+  std::vector<BatchItem> items;
+  int nchain = 1;
+  std::vector<void *> T;
+  std::vector<size_t> Tbytes;
+  std::vector<unsigned int *> sync;
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> joins;
+  cudaEvent_t fork = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t last = nullptr;
+  std::vector<float> tuned_ms;          // per plan: best time of the chosen variant (tuning on)
+  std::vector<int> variant;             // per plan: 2 * (s1_nt == 256) + (persistent stage 2)
+};
+
+void batch_free(Batch *b)
+{
+  if (!b) return;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(b->device);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  for (void *t : b->T) if (t) cudaFree(t);
+  for (unsigned int *q : b->sync) if (q) cudaFree(q);
+  for (cudaStream_t s : b->streams) if (s) cudaStreamDestroy(s);
+  for (cudaEvent_t e : b->joins) if (e) cudaEventDestroy(e);
+  if (b->fork) cudaEventDestroy(b->fork);
+  for (Plan *p : b->plans) free_plan(p);
+  cudaSetDevice(cur);
+  delete b;
+}
+
+// enqueue one transform of the batch on its chain's stream
+int batch_enqueue(Batch &b, const BatchItem &it)
+{
+  Plan &p = *b.plans[it.plan];
+  const Exec ex{ it.in, b.T[it.chain], it.out, b.sync[it.chain], it.lo, it.hi, b.streams[it.chain] };
+  int rc;
+  if ((rc = run_stage1(p, ex))) return rc;
+  if (b.tmpl.use_vlc && (rc = run_vlc(p, ex))) return rc;
+  return run_stage2(p, ex);
+}
+
+// time one plan variant on a transform (min of `reps` runs after a warm-up)
+int batch_time_variant(Batch &b, Plan &p, const BatchItem &it, void *out, float *ms)
+{
+  cudaStream_t st = b.streams[0];
+  const Exec ex{ it.in, b.T[0], out, b.sync[0], it.lo, it.hi, st };
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int rc = SOI_OK;
+  for (int r = 0; r < 4 && rc == SOI_OK; ++r) {
+    CK(cudaEventRecord(e0, st));
+    rc = run_stage1(p, ex);
+    if (rc == SOI_OK && b.tmpl.use_vlc) rc = run_vlc(p, ex);
+    if (rc == SOI_OK) rc = run_stage2(p, ex);
+    CK(cudaEventRecord(e1, st));
+    CK(cudaEventSynchronize(e1));
+    float t = 0;
+    cudaEventElapsedTime(&t, e0, e1);
+    if (r > 0) best = std::min(best, t);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc == SOI_OK) rc = check_stage2(p, b.sync[0], st);
+  *ms = best;
+  return rc;
+}
+
+int batch_build(Batch &b, int tune)
+{
+  // plans: one per distinct (N, k); tuning picks the fastest variant
+  std::vector<std::pair<size_t, size_t>> shapes;
+  for (auto &it : b.items) {
+    size_t i = 0;
+    while (i < shapes.size() && !(shapes[i].first == it.N && shapes[i].second == it.k)) ++i;
+    if (i == shapes.size()) shapes.push_back({ it.N, it.k });
+    it.plan = (int)i;
+  }
+  b.nchain = std::max(1, std::min(b.nchain, (int)b.items.size()));
+  if (b.tmpl.use_vlc) b.nchain = 1;              // VLC buffers belong to the plan
+  // chains: largest transforms first onto the least-loaded chain
+  std::vector<int> order(b.items.size());
+  for (size_t i = 0; i < order.size(); ++i) {
+    order[i] = (int)i;
+    BatchItem &it = b.items[i];
+    it.work = (double)it.N * std::log2((double)it.N);
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return b.items[x].work > b.items[y].work; });
+  std::vector<double> load(b.nchain, 0.0);
+  std::vector<size_t> tmax(b.nchain, 0), smax(b.nchain, 0);
+  for (int i : order) {
+    int c = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    BatchItem &it = b.items[i];
+    it.chain = c;
+    load[c] += it.work;
+    const size_t Mh = (size_t)b.tmpl.n_mu * (it.N / it.k) / (size_t)b.tmpl.d_mu;
+    const size_t elem = b.tmpl.precision == SOI_PRECISION_FP64 ? 16 : 8;
+    tmax[c] = std::max(tmax[c], it.k * Mh * elem);
+    smax[c] = std::max(smax[c], it.k);
+  }
+  b.T.assign(b.nchain, nullptr);
+  b.Tbytes = tmax;
+  b.sync.assign(b.nchain, nullptr);
+  b.streams.assign(b.nchain, nullptr);
+  b.joins.assign(b.nchain, nullptr);
+  for (int c = 0; c < b.nchain; ++c) {
+    CK(cudaMalloc(&b.T[c], std::max<size_t>(tmax[c], 16)));
+    CK(cudaMalloc(&b.sync[c], (smax[c] + 2) * sizeof(unsigned int)));
+    CK(cudaMemset(b.sync[c], 0, (smax[c] + 2) * sizeof(unsigned int)));
+    CK(cudaStreamCreateWithFlags(&b.streams[c], cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&b.joins[c], cudaEventDisableTiming));
+  }
+  CK(cudaEventCreateWithFlags(&b.fork, cudaEventDisableTiming));
+  // tuning needs chain 0's scratch to hold every shape
+  if (tune) {
+    size_t need = 0;
+    for (auto &it : b.items)
+      need = std::max(need, it.k * ((size_t)b.tmpl.n_mu * (it.N / it.k) / (size_t)b.tmpl.d_mu) *
+                                (b.tmpl.precision == SOI_PRECISION_FP64 ? 16 : 8));
+    if (need > tmax[0]) {
+      CK(cudaFree(b.T[0]));
+      CK(cudaMalloc(&b.T[0], need));
+      tmax[0] = need;
+      b.Tbytes[0] = need;
+    }
+    size_t kmax = 0;
+    for (auto &it : b.items) kmax = std::max(kmax, it.k);
+    if (kmax > smax[0]) {
+      CK(cudaFree(b.sync[0]));
+      CK(cudaMalloc(&b.sync[0], (kmax + 2) * sizeof(unsigned int)));
+      CK(cudaMemset(b.sync[0], 0, (kmax + 2) * sizeof(unsigned int)));
+    }
+  }
+  void *scratch_out = nullptr;
+  if (tune) {
+    size_t nmax = 0;
+    for (auto &it : b.items) nmax = std::max(nmax, it.N);
+    CK(cudaMalloc(&scratch_out, nmax * (b.tmpl.precision == SOI_PRECISION_FP64 ? 16 : 8)));
+  }
+  int rc = SOI_OK;
+  for (size_t si = 0; si < shapes.size() && rc == SOI_OK; ++si) {
+    soi_desc_t d = b.tmpl;
+    d.N = shapes[si].first;
+    const BatchItem *first = nullptr;
+    for (auto &it : b.items) if (it.plan == (int)si) { first = &it; break; }
+    Plan *best = nullptr;
+    float best_ms = 0;
+    int best_var = 0;
+    const int nts[2] = { 256, 512 }, s2s[2] = { 1, 0 };
+    std::vector<int> tried;             // variant signatures already timed
+    for (int a = 0; a < (tune ? 2 : 1) && rc == SOI_OK; ++a)
+      for (int c = 0; c < (tune ? 2 : 1) && rc == SOI_OK; ++c) {
+        Plan *p = nullptr;
+        rc = make_plan(&d, shapes[si].second, tune ? nts[a] : -1, tune ? s2s[c] : -1, false, &p);
+        if (rc) break;
+        if (b.tmpl.use_vlc && (rc = vlc_alloc(*p))) { free_plan(p); break; }
+        if (!tune) { best = p; break; }
+        // a shape without a given variant falls back to another one: time each
+        // distinct kernel choice once
+        const int sig = (p->s1fast ? 1 : 0) + 2 * p->s1_tS + 4 * (p->s1_nt == 256) + 8 * (p->fast2 ? 1 : 0);
+        if (std::find(tried.begin(), tried.end(), sig) != tried.end()) { free_plan(p); continue; }
+        tried.push_back(sig);
+        float ms = 0;
+        rc = batch_time_variant(b, *p, *first, scratch_out, &ms);
+        if (rc) { free_plan(p); break; }
+        if (!best || ms < best_ms) {
+          if (best) free_plan(best);
+          best = p; best_ms = ms; best_var = 2 * (p->s1_nt == 256) + (p->fast2 ? 1 : 0);
+        } else {
+          free_plan(p);
+        }
+      }
+    if (rc) { if (best) free_plan(best); break; }
+    b.plans.push_back(best);
+    b.tuned_ms.push_back(best_ms);
+    b.variant.push_back(tune ? best_var : 2 * (best->s1_nt == 256) + (best->fast2 ? 1 : 0));
+  }
+  if (scratch_out) cudaFree(scratch_out);
+  if (rc) return rc;
+  CK(cudaDeviceSynchronize());
+  // capture: fork every chain from the capture stream, enqueue, join
+  cudaStream_t cap = nullptr;
+  CK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+  rc = SOI_OK;
+  if (cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess) rc = SOI_ERR_CUDA;
+  if (rc == SOI_OK && cudaEventRecord(b.fork, cap) != cudaSuccess) rc = SOI_ERR_CUDA;
+  for (int c = 0; c < b.nchain && rc == SOI_OK; ++c) {
+    if (cudaStreamWaitEvent(b.streams[c], b.fork, 0) != cudaSuccess) { rc = SOI_ERR_CUDA; break; }
+    // the error flag of a chain starts clear at every launch of the graph
+    if (cudaMemsetAsync(b.sync[c], 0, sizeof(unsigned int), b.streams[c]) != cudaSuccess) rc = SOI_ERR_CUDA;
+  }
+  for (size_t i = 0; i < b.items.size() && rc == SOI_OK; ++i) rc = batch_enqueue(b, b.items[i]);
+  for (int c = 0; c < b.nchain && rc == SOI_OK; ++c) {
+    if (cudaEventRecord(b.joins[c], b.streams[c]) != cudaSuccess ||
+        cudaStreamWaitEvent(cap, b.joins[c], 0) != cudaSuccess) rc = SOI_ERR_CUDA;
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(cap, &g);
+  cudaStreamDestroy(cap);
+  if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+  if (ce != cudaSuccess || !g) return SOI_ERR_CUDA;
+  b.graph = g;
+  CK(cudaGraphInstantiate(&b.exec, b.graph, 0));
+  return SOI_OK;
 }
 
 }  // namespace
@@ -1024,6 +1292,7 @@ int soi_segment_fft_demod_device(soi_desc_t *d, void *T_dev, void *out_dev)
   if (!p) return SOI_ERR_NOT_INITIALISED;
   if (cudaSetDevice(p->device) != cudaSuccess) return SOI_ERR_CUDA;
   const Exec ex{ nullptr, T_dev, out_dev, p->d_sync, 0, (int)p->S, p->stream };
+  if (p->fast2) CK(cudaMemsetAsync(p->d_sync, 0, sizeof(unsigned int), p->stream));
   int rc = run_stage2(*p, ex);
   if (rc == SOI_OK) rc = check_stage2(*p, p->d_sync, p->stream);
   return rc;
@@ -1157,6 +1426,110 @@ int soi_vlc_decompress_device(const int *words, long stride_words, int len, int 
   CK(cudaGetLastError());
   CK(cudaFreeAsync(d_emax, (cudaStream_t)stream));
   CK(cudaStreamSynchronize((cudaStream_t)stream));
+  return SOI_OK;
+}
+
+int soi_batch_create(soi_batch_t **batch, const soi_desc_t *tmpl, const soi_batch_item_t *items, int count,
+                     int chains, int tune)
+{
+  if (!batch || !tmpl || !items || count < 1 || chains < 1) return SOI_ERR_INVALID;
+  *batch = nullptr;
+  Batch *b = new Batch();
+  b->tmpl = *tmpl;
+  b->tmpl.plan = nullptr;
+  b->tmpl.segmentBoundaries = nullptr;
+  b->tmpl.P = 1;
+  b->tmpl.rank = 0;
+  b->device = tmpl->device;
+  b->nchain = chains;
+  for (int i = 0; i < count; ++i) {
+    const soi_batch_item_t &x = items[i];
+    if (!x.in || !x.out || x.k < 1) { delete b; return SOI_ERR_INVALID; }
+    BatchItem it;
+    it.N = x.N; it.k = x.k; it.in = x.in; it.out = x.out;
+    it.lo = x.seg_hi <= 0 ? 0 : x.seg_lo;
+    it.hi = x.seg_hi <= 0 ? (int)x.k : x.seg_hi;
+    if (it.lo < 0 || it.hi > (int)x.k || it.lo >= it.hi) { delete b; return SOI_ERR_INVALID; }
+    soi_desc_t d = b->tmpl;
+    d.N = x.N;
+    int rc = validate(&d, x.k);
+    if (rc) { delete b; return rc; }
+    b->items.push_back(it);
+  }
+  if (cudaSetDevice(b->device) != cudaSuccess) { delete b; return SOI_ERR_CUDA; }
+  int rc = batch_build(*b, tune);
+  if (rc) { batch_free(b); return rc; }
+  *batch = (soi_batch_t *)b;
+  return SOI_OK;
+}
+
+int soi_batch_execute(soi_batch_t *batch, void *stream)
+{
+  Batch *b = (Batch *)batch;
+  if (!b || !b->exec) return SOI_ERR_NOT_INITIALISED;
+  if (cudaSetDevice(b->device) != cudaSuccess) return SOI_ERR_CUDA;
+  CK(cudaGraphLaunch(b->exec, (cudaStream_t)stream));
+  b->last = (cudaStream_t)stream;
+  return SOI_OK;
+}
+
+int soi_batch_check(soi_batch_t *batch)
+{
+  Batch *b = (Batch *)batch;
+  if (!b) return SOI_ERR_NOT_INITIALISED;
+  if (cudaSetDevice(b->device) != cudaSuccess) return SOI_ERR_CUDA;
+  CK(cudaStreamSynchronize(b->last));
+  for (int c = 0; c < b->nchain; ++c) {
+    unsigned int err = 0;
+    CK(cudaMemcpy(&err, b->sync[c], sizeof(err), cudaMemcpyDeviceToHost));
+    if (err) return SOI_ERR_TIMEOUT;
+  }
+  return SOI_OK;
+}
+
+int soi_batch_info(soi_batch_t *batch, long long *info)
+{
+  Batch *b = (Batch *)batch;
+  if (!b || !info) return SOI_ERR_INVALID;
+  size_t nodes = 0;
+  if (b->graph) cudaGraphGetNodes(b->graph, nullptr, &nodes);
+  info[0] = (long long)b->items.size();
+  info[1] = (long long)b->plans.size();
+  info[2] = b->nchain;
+  info[3] = (long long)nodes;
+  long long launches = 0;
+  for (auto &it : b->items) {
+    const Plan &p = *b->plans[it.plan];
+    launches += 1 + (p.fast2 ? 1 : 2) + (b->tmpl.use_vlc ? (p.prec == SOI_PRECISION_FP64 ? 4 : 6) : 0);
+  }
+  info[4] = launches;
+  size_t scratch = 0;
+  for (size_t t : b->Tbytes) scratch += t;
+  info[5] = (long long)scratch;
+  info[6] = 0;
+  info[7] = 0;
+  return SOI_OK;
+}
+
+int soi_batch_plan_info(soi_batch_t *batch, int plan, long long *info)
+{
+  Batch *b = (Batch *)batch;
+  if (!b || !info || plan < 0 || plan >= (int)b->plans.size()) return SOI_ERR_INVALID;
+  const Plan &p = *b->plans[plan];
+  info[0] = (long long)p.N;
+  info[1] = (long long)p.S;
+  info[2] = p.s1fast ? (p.s1_tS ? p.s1_nt : 512) : 256;
+  info[3] = p.fast2 ? 1 : 0;
+  info[4] = p.M1;
+  info[5] = p.M2;
+  info[6] = (long long)(b->tuned_ms[plan] * 1000.0f);
+  info[7] = b->variant[plan];
+  return SOI_OK;
+}
+
+int soi_batch_destroy(soi_batch_t *batch)
+{
+  batch_free((Batch *)batch);
   return SOI_OK;
 }
 

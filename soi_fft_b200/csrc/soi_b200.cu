@@ -535,11 +535,13 @@ void plan_stage1_staged(Plan &p)
   const int jr = staged_jr(p.prec, p.nmu);
   if (!jr || p.S > 512 || (p.S * p.nmu) % 4) return;
   const bool ts = tS_available(p);
-  // compile-time-S kernel: 256 threads and <= 110 KB (two CTAs per SM) where
-  // a tile of at least two thread rows fits, else 512 threads and 200 KB
+  // compile-time-S kernel: 512 threads and 200 KB (one CTA per SM), or 256
+  // threads and <= 110 KB (two CTAs per SM, smaller tiles: more halo rows per
+  // output) where two thread rows fit.  512 measured faster at N = 2^29,
+  // S = 128 (6.64 vs 7.25 ms); the batch tuner tries both.
   int nt = 512;
   if (ts && 2 * (int)p.S <= 256)
-    nt = (p.knob_s1_nt > 0 ? p.knob_s1_nt : env_int("SOI_STAGE1_NT", 256)) == 512 ? 512 : 256;
+    nt = (p.knob_s1_nt > 0 ? p.knob_s1_nt : env_int("SOI_STAGE1_NT", 512)) == 256 ? 256 : 512;
   const int groups = nt / (int)p.S;
   const size_t budget = (nt == 256 ? 110 * 1024 : 200 * 1024) - p.S * (p.elem + sizeof(int));
   const size_t real = p.elem / 2;

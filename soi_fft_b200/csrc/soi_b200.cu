@@ -55,6 +55,7 @@ struct Plan {
   int f2_grid = 0;
   size_t f2_smem = 0;
   int discard = 1;             // drop consumed intermediate lines from L2
+  int wait_extra = 0;          // failure test: pass-2 waits for a count that never comes
   void *d_amp = nullptr;            // [M/2+1] real demodulation amplitude
   double2 *d_dlo = nullptr, *d_dhi = nullptr;
   int dlo_bits = 11;
@@ -402,6 +403,10 @@ int setup_s2ct(Plan &p, int idx)
   int rc = p.prec == SOI_PRECISION_FP64 ? build_demod_tables<double>(p, true) : build_demod_tables<float>(p, true);
   if (rc) return rc;
   p.discard = env_int("SOI_STAGE2_DISCARD", 1);
+  // failure-detection test only: every pass-2 task then waits for one more
+  // pass-1 completion than exists, runs out its iteration limit and the
+  // compute returns SOI_ERR_TIMEOUT
+  p.wait_extra = env_int("SOI_TEST_STAGE2_WAIT_EXTRA", 0) ? 1 : 0;
   p.fast2 = 3;
   return SOI_OK;
 }
@@ -414,6 +419,7 @@ int launch_s2ct(Plan &p, const Exec &ex)
   a.lo_bits = p.lo_bits; a.dlo_bits = p.dlo_bits; a.M = (int)p.M;
   a.S = ex.hi - ex.lo; a.seg_lo = ex.lo;
   a.discard = p.discard;
+  a.wait_extra = p.wait_extra;
   a.err = (int *)ex.sync; a.counter = ex.sync + 1; a.done1 = ex.sync + 2;
   // counters restart; the error flag stays set until the owner clears it
   CK(cudaMemsetAsync(ex.sync + 1, 0, (size_t)(a.S + 1) * sizeof(unsigned int), ex.st));

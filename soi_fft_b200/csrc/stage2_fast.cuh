@@ -92,6 +92,7 @@ struct S2ArgsCT {
   int S;                      // segments in this launch
   int seg_lo;                 // first segment of this launch
   int discard;
+  int wait_extra;             // 0; a test sets 1 to make every pass-2 wait run out
   unsigned int *counter, *done1;
   int *err;
 };
@@ -193,8 +194,9 @@ __global__ void __launch_bounds__(NT, 2) k_stage2_ct(S2ArgsCT a)
         const int blk = (int)(u / G::PER), r = (int)(u % G::PER);
         if (blk >= a.S - 1 || r >= G::NT1) {                // pass-2 task of segment blk
           long long it = 0;
-          while (ld_acquire_u32(a.done1 + blk) < (unsigned int)G::NT1) {
+          while (ld_acquire_u32(a.done1 + blk) < (unsigned int)(G::NT1 + a.wait_extra)) {
             if (++it > kWaitLimit) { atomicExch(a.err, 1); ok = 0; break; }
+            if (*(volatile int *)a.err) { ok = 0; break; }   // another CTA gave up
             __nanosleep(128);
           }
         }

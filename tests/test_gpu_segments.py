@@ -124,3 +124,29 @@ def test_async_compute_captures_into_a_cuda_graph(N, S, prec):
         del g
     finally:
         d.free()
+
+
+def test_stage2_wait_that_runs_out_reports_timeout_and_leaves_the_gpu_usable(monkeypatch):
+    # failure detection without a fault: the plan is told to wait for one more
+    # pass-1 completion than exists, so every pass-2 wait gives up after its
+    # iteration limit; the kernel returns, the host reads the error flag
+    N, S, prec = 1 << 20, 16, sb.PRECISION_SPLIT_FP32
+    x = _input(N, prec)
+    monkeypatch.setenv("SOI_TEST_STAGE2_WAIT_EXTRA", "1")
+    d = _desc(N, S, prec)
+    monkeypatch.delenv("SOI_TEST_STAGE2_WAIT_EXTRA")
+    try:
+        y = torch.empty_like(x)
+        with pytest.raises(sb.SoiError) as e:
+            d.compute_into(x, y)
+        assert e.value.status == 5          # SOI_ERR_TIMEOUT
+    finally:
+        d.free()
+    d2 = _desc(N, S, prec)
+    try:
+        y = torch.empty_like(x)
+        d2.compute_into(x, y)
+        X = torch.fft.fft(x.to(torch.complex128))
+        assert float(torch.linalg.norm(y.to(torch.complex128) - X) / torch.linalg.norm(X)) < 1e-6
+    finally:
+        d2.free()

@@ -115,6 +115,14 @@ int soi_compute_segments_status(soi_desc_t *desc, const void *in, void *out, int
  * recorded into a CUDA graph.  A persistent-kernel wait that gave up is
  * reported by the next soi_check_status.  No counterpart in the reference. */
 int soi_compute_async_status(soi_desc_t *desc, const void *in, void *out);
+/* Several transforms of host buffers (device_ptr = 0): outs[i] receives the
+ * transform of ins[i], i < count.  Uploads, kernels and downloads of
+ * neighbouring transforms overlap on separate streams (PCIe carries both
+ * directions at once), so with pinned buffers the cost per transform
+ * approaches one copy time instead of two plus the kernels.  Two N-element
+ * device staging buffers, allocated on first use.  Returns after the last
+ * download.  No counterpart in the reference. */
+int soi_compute_stream_status(soi_desc_t *desc, const void *const *ins, void *const *outs, int count);
 /* Waits for the descriptor's stream and returns SOI_ERR_TIMEOUT if a
  * stage-2 dependency wait gave up since the last compute, else SOI_OK. */
 int soi_check_status(soi_desc_t *desc);

@@ -65,6 +65,8 @@ def lib():
         L.soi_compute_segments_status.argtypes = [P, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
         L.soi_compute_async_status.argtypes = [P, ctypes.c_void_p, ctypes.c_void_p]
         L.soi_check_status.argtypes = [P]
+        L.soi_compute_stream_status.argtypes = [P, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p),
+                                                ctypes.c_int]
         L.soi_free_status.argtypes = [P]
         L.set_default_soi_descriptor.argtypes = [P]
         L.soi_status_string.restype = ctypes.c_char_p
@@ -212,6 +214,22 @@ class SoiDescriptor:
         px, po = self._ptr(x), self._ptr(out)
         _check(lib().soi_compute_async_status(ctypes.byref(self._d), px, po), "soi_compute_async")
         return out
+
+    def compute_stream(self, xs, ys):
+        """Transforms of several host arrays, ys[i] <- transform of xs[i], with
+        the uploads, kernels and downloads of neighbours overlapped (pinned
+        host memory makes the copies overlap)."""
+        if len(xs) != len(ys) or not xs:
+            raise ValueError("xs and ys must be non-empty lists of the same length")
+        ins = (ctypes.c_void_p * len(xs))()
+        outs = (ctypes.c_void_p * len(ys))()
+        for i, (x, y) in enumerate(zip(xs, ys)):
+            if _is_torch_cuda(x) or _is_torch_cuda(y):
+                raise ValueError("compute_stream takes host arrays")
+            ins[i] = self._ptr(x)
+            outs[i] = self._ptr(y)
+        _check(lib().soi_compute_stream_status(ctypes.byref(self._d), ins, outs, len(xs)), "soi_compute_stream")
+        return ys
 
     def check(self):
         """Wait for the descriptor's stream; raise if a stage-2 wait gave up."""

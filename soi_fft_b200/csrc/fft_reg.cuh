@@ -194,14 +194,16 @@ __device__ __forceinline__ void tile_fft_ct(V *sm, const V *__restrict__ tw, con
     for (int q = threadIdx.x; q < n; q += NT) {
       const int col = q % C, blk = q / C;
       const V *p = sm + blk * DL + col * PC;
+      int fbase;
+      if constexpr (R2 > 1) fbase = (blk / R1) + R0 * (blk % R1);
+      else fbase = blk;
+      // the epilogue's own loads go out before the last radix's arithmetic
+      const auto pre = emit.prepare(col, fbase);
       V v[RL];
 #pragma unroll
       for (int r = 0; r < RL; ++r) v[r] = p[r * PP];
       RegDFT<V, RL>::run(v);
-      int fbase;
-      if constexpr (R2 > 1) fbase = (blk / R1) + R0 * (blk % R1);
-      else fbase = blk;
-      emit.template run<RL>(col, fbase, L / RL, v);
+      emit.template run<RL>(col, fbase, L / RL, v, pre);
     }
   }
 }

@@ -45,6 +45,9 @@ struct Plan {
   double2 *d_xlo = nullptr, *d_xhi = nullptr;
   void *d_T = nullptr;         // S*Mh complex
   void *d_io = nullptr;        // N complex staging for host pointers
+  void *d_io2 = nullptr;       // second staging buffer (streamed host transforms)
+  cudaStream_t st_in = nullptr, st_out = nullptr;   // copy streams (streamed host transforms)
+  cudaEvent_t sev[6] = {};     // in-copied[2], computed[2], out-copied[2]
   // VLC
   double *d_vlc_x = nullptr;   // promoted/decompressed doubles (FP32 path)
   int *d_vlc_words = nullptr, *d_vlc_n = nullptr, *d_vlc_emax = nullptr;
@@ -700,10 +703,13 @@ void free_plan(Plan *p)
   cudaGetDevice(&cur);
   cudaSetDevice(p->device);
   void *bufs[] = { p->d_filt, p->d_phase, p->d_twS, p->d_tw1, p->d_tw2, p->d_winv, p->d_wsmall,
-                   p->d_permS, p->d_perm1, p->d_perm2, p->d_xlo, p->d_xhi, p->d_T, p->d_io,
+                   p->d_permS, p->d_perm1, p->d_perm2, p->d_xlo, p->d_xhi, p->d_T, p->d_io, p->d_io2,
                    p->d_vlc_x, p->d_vlc_words, p->d_vlc_n, p->d_vlc_emax, p->d_sync, p->d_filt2, p->d_amp, p->d_dlo, p->d_dhi, p->d_ph2 };
   for (void *b : bufs) if (b) cudaFree(b);
   for (auto &e : p->ev) if (e) cudaEventDestroy(e);
+  for (auto &e : p->sev) if (e) cudaEventDestroy(e);
+  if (p->st_in) cudaStreamDestroy(p->st_in);
+  if (p->st_out) cudaStreamDestroy(p->st_out);
   if (p->own_stream && p->stream) cudaStreamDestroy(p->stream);
   cudaSetDevice(cur);
   delete p;
@@ -1232,10 +1238,70 @@ int soi_compute_segments_status(soi_desc_t *d, const void *in, void *out, int se
   return rc;
 }
 
+// Streamed host transforms: ins[i] -> outs[i] for i < count, host buffers
+// (pinned for the copies to overlap).  Two device staging buffers; transform
+// i's upload (copy stream in), kernels (the plan's stream) and download (copy
+// stream out) overlap with its neighbours', so PCIe carries both directions
+// at once.  Each transform runs in place in its staging buffer; a buffer is
+// refilled only after its previous download finished.
+int compute_stream_impl(soi_desc_t *d, const void *const *ins, void *const *outs, int count)
+{
+  Plan *p = plan_of(d);
+  if (!p) return SOI_ERR_NOT_INITIALISED;
+  if (count < 1 || !ins || !outs) return SOI_ERR_INVALID;
+  for (int i = 0; i < count; ++i) if (!ins[i] || !outs[i]) return SOI_ERR_INVALID;
+  if (cudaSetDevice(p->device) != cudaSuccess) return SOI_ERR_CUDA;
+  const size_t bytes = p->N * p->elem;
+  if (!p->d_io) CK(cudaMalloc(&p->d_io, bytes));
+  if (!p->d_io2) CK(cudaMalloc(&p->d_io2, bytes));
+  if (!p->st_in) CK(cudaStreamCreateWithFlags(&p->st_in, cudaStreamNonBlocking));
+  if (!p->st_out) CK(cudaStreamCreateWithFlags(&p->st_out, cudaStreamNonBlocking));
+  for (auto &e : p->sev)
+    if (!e) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  cudaStream_t st = p->stream;
+  void *buf[2] = { p->d_io, p->d_io2 };
+  cudaEvent_t *in_done = p->sev, *comp_done = p->sev + 2, *out_done = p->sev + 4;
+  if (p->fast2) CK(cudaMemsetAsync(p->d_sync, 0, sizeof(unsigned int), st));
+  // the copy streams start after everything already queued on the plan's stream
+  CK(cudaEventRecord(comp_done[0], st));
+  CK(cudaStreamWaitEvent(p->st_in, comp_done[0], 0));
+  CK(cudaStreamWaitEvent(p->st_out, comp_done[0], 0));
+  for (int i = 0; i < count; ++i) {
+    const int b = i & 1;
+    if (i >= 2) CK(cudaStreamWaitEvent(p->st_in, out_done[b], 0));   // buffer b drained
+    CK(cudaMemcpyAsync(buf[b], ins[i], bytes, cudaMemcpyHostToDevice, p->st_in));
+    CK(cudaEventRecord(in_done[b], p->st_in));
+    CK(cudaStreamWaitEvent(st, in_done[b], 0));
+    const Exec ex{ buf[b], p->d_T, buf[b], p->d_sync, 0, (int)p->S, st };
+    int rc;
+    if ((rc = run_stage1(*p, ex))) return rc;
+    if (d->use_vlc && (rc = run_vlc(*p, ex))) return rc;
+    if ((rc = run_stage2(*p, ex))) return rc;
+    CK(cudaEventRecord(comp_done[b], st));
+    CK(cudaStreamWaitEvent(p->st_out, comp_done[b], 0));
+    CK(cudaMemcpyAsync(outs[i], buf[b], bytes, cudaMemcpyDeviceToHost, p->st_out));
+    CK(cudaEventRecord(out_done[b], p->st_out));
+  }
+  // the plan's stream ends after the last download
+  CK(cudaStreamWaitEvent(st, out_done[(count - 1) & 1], 0));
+  CK(cudaStreamSynchronize(st));
+  CK(cudaStreamSynchronize(p->st_out));
+  return check_stage2(*p, p->d_sync, st);
+}
+
 int soi_compute_async_status(soi_desc_t *d, const void *in, void *out)
 {
   if (!d) return SOI_ERR_INVALID;
   int rc = (in && out) ? compute_impl(d, in, out, false, 0, -1, false) : SOI_ERR_INVALID;
+  d->last_status = rc;
+  return rc;
+}
+
+int soi_compute_stream_status(soi_desc_t *d, const void *const *ins, void *const *outs, int count)
+{
+  if (!d) return SOI_ERR_INVALID;
+  if (d->device_ptr) return SOI_ERR_INVALID;                     // host buffers only
+  int rc = compute_stream_impl(d, ins, outs, count);
   d->last_status = rc;
   return rc;
 }

@@ -185,9 +185,12 @@ __global__ void __launch_bounds__(512, 1) k_conv_sfft_staged(Conv2Args a)
 // Stores of the tile FFT's last stage: T[f][rho0 + col] (the transposed
 // store of .cpp:391 / the all-to-all of pfft.c:554-578), consecutive threads
 // on consecutive rows rho.
+struct NoPrep {};
+
 template <typename V> struct EmitTransposed {
   V *T; long long Mh, rho0; int lo, hi;   // segments f in [lo, hi) are stored
-  template <int RL> __device__ __forceinline__ void run(int col, int fbase, int fstep, V *v) const
+  __device__ __forceinline__ NoPrep prepare(int, int) const { return NoPrep{}; }
+  template <int RL> __device__ __forceinline__ void run(int col, int fbase, int fstep, V *v, NoPrep = NoPrep{}) const
   {
     const long long rho = rho0 + col;
     if (rho < Mh) {

@@ -107,11 +107,15 @@ __device__ __forceinline__ V two_level(const double2 *lo, const double2 *hi, int
 
 template <typename V, int C1, int M2, int RL> struct EmitColsCT {
   V *Tseg; int m2_0; const V *step; const S2ArgsCT *a;
-  template <int RLx> __device__ __forceinline__ void run(int col, int fbase, int fstep, V *v) const
+  // w_{M'}^(m2*fbase), loaded and formed before the last radix
+  __device__ __forceinline__ V prepare(int col, int fbase) const
+  {
+    return two_level<V>(a->xlo, a->xhi, a->lo_bits, (m2_0 + col) * fbase);
+  }
+  template <int RLx> __device__ __forceinline__ void run(int col, int fbase, int fstep, V *v, V base) const
   {
     static_assert(RLx == RL, "last radix");
     const int m2 = m2_0 + col;
-    const V base = two_level<V>(a->xlo, a->xhi, a->lo_bits, m2 * fbase);
     V *dst = Tseg + fbase * M2 + m2;
     dst[0] = cmul(v[0], base);
 #pragma unroll
@@ -119,9 +123,12 @@ template <typename V, int C1, int M2, int RL> struct EmitColsCT {
   }
 };
 
+struct NoPre {};
+
 template <typename V, int M1, int RL> struct EmitRowsCT {
   V *oseg; int k1_0; const V *ph1; const S2ArgsCT *a;
-  template <int RLx> __device__ __forceinline__ void run(int col, int fbase, int fstep, V *v) const
+  __device__ __forceinline__ NoPre prepare(int, int) const { return NoPre{}; }
+  template <int RLx> __device__ __forceinline__ void run(int col, int fbase, int fstep, V *v, NoPre) const
   {
     static_assert(RLx == RL, "last radix");
     using Rr = decltype(V::x);
@@ -130,14 +137,32 @@ template <typename V, int M1, int RL> struct EmitRowsCT {
     const V p1 = ph1[col];
     const V *ph2 = reinterpret_cast<const V *>(a->ph2);
     const Rr *amp = reinterpret_cast<const Rr *>(a->amp);
+    // every load in bounds (discarded bins read amp[0]), so the loads do not
+    // wait on the discard test
+    if constexpr (sizeof(V) == 8) {
+      // FP32: all RL factors in flight before the first store
+      V w[RL];
 #pragma unroll
-    for (int j = 0; j < RL; ++j) {
-      const int k2 = fbase + fstep * j;
-      const int k = k1 + M1 * k2;
-      if (k < M) {
-        const int km = k <= M - k ? k : M - k;
+      for (int j = 0; j < RL; ++j) {
+        const int k2 = fbase + fstep * j;
+        const int k = k1 + M1 * k2;
+        const int km = k >= M ? 0 : (k <= M - k ? k : M - k);
+        w[j] = cscale(cmul(p1, __ldg(ph2 + k2)), __ldg(amp + km));
+      }
+#pragma unroll
+      for (int j = 0; j < RL; ++j) {
+        const int k = k1 + M1 * (fbase + fstep * j);
+        if (k < M) stcs(oseg + k, cmul(v[j], w[j]));
+      }
+    } else {
+      // FP64: RL double factors would not fit in registers beside the data
+#pragma unroll
+      for (int j = 0; j < RL; ++j) {
+        const int k2 = fbase + fstep * j;
+        const int k = k1 + M1 * k2;
+        const int km = k >= M ? 0 : (k <= M - k ? k : M - k);
         const V w = cscale(cmul(p1, __ldg(ph2 + k2)), __ldg(amp + km));
-        stcs(oseg + k, cmul(v[j], w));
+        if (k < M) stcs(oseg + k, cmul(v[j], w));
       }
     }
   }

@@ -150,3 +150,30 @@ def test_stage2_wait_that_runs_out_reports_timeout_and_leaves_the_gpu_usable(mon
         assert float(torch.linalg.norm(y.to(torch.complex128) - X) / torch.linalg.norm(X)) < 1e-6
     finally:
         d2.free()
+
+
+@pytest.mark.parametrize("pinned", [True, False])
+@pytest.mark.parametrize("N,S,prec", [(1 << 20, 16, sb.PRECISION_SPLIT_FP32), (1 << 18, 8, sb.PRECISION_FP64)])
+def test_streamed_host_transforms_equal_single_computes(N, S, prec, pinned):
+    dt = np.complex64 if prec == sb.PRECISION_SPLIT_FP32 else np.complex128
+    tdt = torch.complex64 if prec == sb.PRECISION_SPLIT_FP32 else torch.complex128
+
+    def host(a):
+        if not pinned:
+            return np.ascontiguousarray(a)
+        t = torch.empty(a.size, dtype=tdt, pin_memory=True)
+        v = t.numpy()
+        v[:] = a
+        return v
+
+    xs = [host(signals.gaussian(N, 20 + i).astype(dt)) for i in range(5)]
+    ys = [host(np.zeros(N, dt)) for _ in range(5)]
+    d = _desc(N, S, prec)
+    try:
+        d.compute_stream(xs, ys)
+        for x, y in zip(xs, ys):
+            ref = np.empty_like(x)
+            d.compute_into(x, ref)
+            assert np.array_equal(y, ref)
+    finally:
+        d.free()

@@ -115,6 +115,11 @@ int soi_compute_segments_status(soi_desc_t *desc, const void *in, void *out, int
  * recorded into a CUDA graph.  A persistent-kernel wait that gave up is
  * reported by the next soi_check_status.  No counterpart in the reference. */
 int soi_compute_async_status(soi_desc_t *desc, const void *in, void *out);
+/* Inverse transform: out[n] = (1/N) sum_k in[k] exp(+2 pi i k n / N), computed
+ * as conj(forward(conj(in)))/N with the same plan (window, precision,
+ * segments); `in` is left untouched; host or device buffers per device_ptr.
+ * No counterpart in the reference, which has no inverse. */
+int soi_compute_inverse_status(soi_desc_t *desc, const void *in, void *out);
 /* Several transforms of host buffers (device_ptr = 0): outs[i] receives the
  * transform of ins[i], i < count.  Uploads, kernels and downloads of
  * neighbouring transforms overlap on separate streams (PCIe carries both

@@ -65,6 +65,7 @@ def lib():
         L.soi_compute_segments_status.argtypes = [P, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
         L.soi_compute_async_status.argtypes = [P, ctypes.c_void_p, ctypes.c_void_p]
         L.soi_check_status.argtypes = [P]
+        L.soi_compute_inverse_status.argtypes = [P, ctypes.c_void_p, ctypes.c_void_p]
         L.soi_compute_stream_status.argtypes = [P, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p),
                                                 ctypes.c_int]
         L.soi_free_status.argtypes = [P]
@@ -213,6 +214,17 @@ class SoiDescriptor:
             raise ValueError("compute_async takes CUDA tensors")
         px, po = self._ptr(x), self._ptr(out)
         _check(lib().soi_compute_async_status(ctypes.byref(self._d), px, po), "soi_compute_async")
+        return out
+
+    def compute_inverse(self, x, out):
+        """Inverse transform x -> out, (1/N) sum_k x[k] exp(+2 pi i k n/N);
+        x is left untouched (both host arrays or both CUDA tensors)."""
+        px = self._ptr(x)
+        dev = self._d.device_ptr
+        po = self._ptr(out)
+        if self._d.device_ptr != dev:
+            raise ValueError("x and out must both be host arrays or both CUDA tensors")
+        _check(lib().soi_compute_inverse_status(ctypes.byref(self._d), px, po), "soi_compute_inverse")
         return out
 
     def compute_stream(self, xs, ys):

@@ -1297,6 +1297,57 @@ int soi_compute_async_status(soi_desc_t *d, const void *in, void *out)
   return rc;
 }
 
+// conj(x) * scale over n complex values on the plan's stream
+int conj_scale(Plan &p, const void *in, void *out, size_t n, double scale, cudaStream_t st)
+{
+  int nsm = 0;
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, p.device));
+  const unsigned grid = (unsigned)std::min<size_t>((n + 255) / 256, (size_t)nsm * 8);
+  if (p.prec == SOI_PRECISION_FP64)
+    k_conj_scale<double><<<grid, 256, 0, st>>>(in, out, (long long)n, scale);
+  else
+    k_conj_scale<float><<<grid, 256, 0, st>>>(in, out, (long long)n, (float)scale);
+  CK(cudaGetLastError());
+  return SOI_OK;
+}
+
+// Inverse transform in -> out: out = conj(in) on the device, the forward
+// transform in place, then out = conj(out) / N.
+int compute_inverse_impl(soi_desc_t *d, const void *in, void *out)
+{
+  Plan *p = plan_of(d);
+  if (!p) return SOI_ERR_NOT_INITIALISED;
+  if (cudaSetDevice(p->device) != cudaSuccess) return SOI_ERR_CUDA;
+  cudaStream_t st = p->stream;
+  const size_t bytes = p->N * p->elem;
+  void *buf = out;
+  if (!d->device_ptr) {
+    if (!p->d_io) CK(cudaMalloc(&p->d_io, bytes));
+    CK(cudaMemcpyAsync(p->d_io, in, bytes, cudaMemcpyHostToDevice, st));
+    buf = p->d_io;
+    in = p->d_io;
+  }
+  int rc;
+  if ((rc = conj_scale(*p, in, buf, p->N, 1.0, st))) return rc;
+  if (p->fast2) CK(cudaMemsetAsync(p->d_sync, 0, sizeof(unsigned int), st));
+  const Exec ex{ buf, p->d_T, buf, p->d_sync, 0, (int)p->S, st };
+  if ((rc = run_stage1(*p, ex))) return rc;
+  if (d->use_vlc && (rc = run_vlc(*p, ex))) return rc;
+  if ((rc = run_stage2(*p, ex))) return rc;
+  if ((rc = conj_scale(*p, buf, buf, p->N, 1.0 / (double)p->N, st))) return rc;
+  if (!d->device_ptr) CK(cudaMemcpyAsync(out, buf, bytes, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return check_stage2(*p, p->d_sync, st);
+}
+
+int soi_compute_inverse_status(soi_desc_t *d, const void *in, void *out)
+{
+  if (!d) return SOI_ERR_INVALID;
+  int rc = (in && out) ? compute_inverse_impl(d, in, out) : SOI_ERR_INVALID;
+  d->last_status = rc;
+  return rc;
+}
+
 int soi_compute_stream_status(soi_desc_t *d, const void *const *ins, void *const *outs, int count)
 {
   if (!d) return SOI_ERR_INVALID;

@@ -247,4 +247,20 @@ __global__ void __launch_bounds__(256) k_seg_rows_demod(SegArgs a)
   }
 }
 
+// ------------------------------------------------------------ inverse --
+// The inverse DFT through the forward pipeline: IDFT(X) = conj(DFT(conj X))/N.
+// out[i] = conj(in[i]) * scale, 16 bytes per thread per step (two complex64
+// values or one complex128), grid-stride.
+template <typename R>
+__global__ void k_conj_scale(const void *in, void *out, long long n, R scale)
+{
+  using V = typename cplx_of<R>::type;
+  const V *x = reinterpret_cast<const V *>(in);
+  V *y = reinterpret_cast<V *>(out);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const V v = x[i];
+    y[i] = cmk<V>(v.x * scale, -v.y * scale);
+  }
+}
+
 }  // namespace soi

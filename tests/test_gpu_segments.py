@@ -177,3 +177,29 @@ def test_streamed_host_transforms_equal_single_computes(N, S, prec, pinned):
             assert np.array_equal(y, ref)
     finally:
         d.free()
+
+
+@pytest.mark.parametrize("N,S,prec,tol", [(1 << 20, 16, sb.PRECISION_SPLIT_FP32, 1e-6),
+                                          (1 << 18, 8, sb.PRECISION_FP64, 1e-12),
+                                          (1 << 22, 32, sb.PRECISION_SPLIT_FP32, 1e-6)])
+def test_inverse_matches_direct_inverse_fft_and_round_trips(N, S, prec, tol):
+    x = _input(N, prec)
+    d = _desc(N, S, prec)
+    try:
+        y = torch.empty_like(x)
+        d.compute_inverse(x, y)
+        ref = torch.fft.ifft(x.to(torch.complex128))
+        assert float(torch.linalg.norm(y.to(torch.complex128) - ref) / torch.linalg.norm(ref)) <= tol
+        # forward then inverse returns the input
+        X = torch.empty_like(x)
+        d.compute_into(x, X)
+        back = torch.empty_like(x)
+        d.compute_inverse(X, back)
+        assert float(torch.linalg.norm((back - x).to(torch.complex128)) / torch.linalg.norm(x.to(torch.complex128))) <= 2 * tol
+        # host buffers
+        xh = x.cpu().numpy()
+        yh = np.empty_like(xh)
+        d.compute_inverse(xh, yh)
+        assert np.array_equal(yh, y.cpu().numpy())
+    finally:
+        d.free()

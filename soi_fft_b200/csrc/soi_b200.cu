@@ -69,15 +69,11 @@ struct Plan {
   int s1fast = 0, JR2 = 0, JT2 = 0, AC = 0, buf_elems = 0;
   int s1_tS = 0;                    // compile-time-S stage-1 instance available
   int s1_nt = 512;                  // its block size (256: two CTAs per SM)
-  int s1_persist = 0;               // persistent compile-time-S stage 1 (cross-tile prefetch)
-  int bufA_elems = 0;               // its region A (output tile or staging buffer)
-  int s1_grid = 0;                  // its grid (one CTA per SM)
   size_t smem1b = 0;
   void *d_filt2 = nullptr;          // [d][atap][nmu][S] real
   // variant choices forced by the batch tuner (-1: defaults / SOI_* switches)
   int knob_s1_nt = -1;              // 256 or 512 threads for the compile-time-S stage 1
   int knob_s2 = -1;                 // 1 persistent stage 2, 0 two-kernel stage 2
-  int knob_s1_persist = -1;         // 1/0: persistent stage 1 or not
   bool timing = false;
   cudaEvent_t ev[5] = {};
   float ms[4] = {0, 0, 0, 0};
@@ -470,7 +466,7 @@ int staged_jr(int prec, int nmu)
   return nmu == 5 ? 4 : nmu == 3 ? 4 : (nmu == 8 || nmu == 9) ? 2 : 0;
 }
 
-template <typename R, int NMU, int JR, int R0, int R1, int NT, bool PERSIST>
+template <typename R, int NMU, int JR, int R0, int R1, int NT>
 int launch_conv_tS(Plan &p, const Exec &ex)
 {
   Conv2Args a;
@@ -479,27 +475,25 @@ int launch_conv_tS(Plan &p, const Exec &ex)
   a.M = (long long)p.M; a.Mh = (long long)p.Mh; a.J = (long long)p.J;
   a.S = (int)p.S; a.d = p.dmu; a.atap = p.atap; a.JT = p.JT2; a.pitch = p.pitch; a.AC = p.AC;
   a.buf_elems = p.buf_elems;
-  a.bufA_elems = p.bufA_elems;
-  auto kern = k_conv_sfft_tS<R, NMU, JR, R0, R1, NT, PERSIST>;
+  auto kern = k_conv_sfft_tS<R, NMU, JR, R0, R1, NT>;
   CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem1b));
-  const long long ntiles = (long long)((p.J + p.JT2 - 1) / p.JT2);
-  dim3 grid((unsigned)(PERSIST ? std::min<long long>(ntiles, p.s1_grid) : ntiles));
+  dim3 grid((unsigned)((p.J + p.JT2 - 1) / p.JT2));
   kern<<<grid, NT, p.smem1b, ex.st>>>(a);
   CK(cudaGetLastError());
   return SOI_OK;
 }
 
 // compile-time-S instances: n_mu = 5, S in {8..256} (R0*R1 split of S)
-template <typename R, int JR, int NT, bool PERSIST>
+template <typename R, int JR, int NT>
 int launch_tS_switch_nt(Plan &p, const Exec &ex)
 {
   switch (p.S) {
-    case 8: return launch_conv_tS<R, 5, JR, 2, 4, NT, PERSIST>(p, ex);
-    case 16: return launch_conv_tS<R, 5, JR, 4, 4, NT, PERSIST>(p, ex);
-    case 32: return launch_conv_tS<R, 5, JR, 4, 8, NT, PERSIST>(p, ex);
-    case 64: return launch_conv_tS<R, 5, JR, 8, 8, NT, PERSIST>(p, ex);
-    case 128: return launch_conv_tS<R, 5, JR, 8, 16, NT, PERSIST>(p, ex);
-    case 256: return launch_conv_tS<R, 5, JR, 16, 16, NT, PERSIST>(p, ex);
+    case 8: return launch_conv_tS<R, 5, JR, 2, 4, NT>(p, ex);
+    case 16: return launch_conv_tS<R, 5, JR, 4, 4, NT>(p, ex);
+    case 32: return launch_conv_tS<R, 5, JR, 4, 8, NT>(p, ex);
+    case 64: return launch_conv_tS<R, 5, JR, 8, 8, NT>(p, ex);
+    case 128: return launch_conv_tS<R, 5, JR, 8, 16, NT>(p, ex);
+    case 256: return launch_conv_tS<R, 5, JR, 16, 16, NT>(p, ex);
   }
   return SOI_ERR_UNSUPPORTED;
 }
@@ -507,8 +501,7 @@ int launch_tS_switch_nt(Plan &p, const Exec &ex)
 template <typename R, int JR>
 int launch_tS_switch(Plan &p, const Exec &ex)
 {
-  if (p.s1_nt == 256) return launch_tS_switch_nt<R, JR, 256, false>(p, ex);
-  return p.s1_persist ? launch_tS_switch_nt<R, JR, 512, true>(p, ex) : launch_tS_switch_nt<R, JR, 512, false>(p, ex);
+  return p.s1_nt == 256 ? launch_tS_switch_nt<R, JR, 256>(p, ex) : launch_tS_switch_nt<R, JR, 512>(p, ex);
 }
 
 bool tS_available(const Plan &p)
@@ -562,31 +555,6 @@ void plan_stage1_staged(Plan &p)
   const size_t budget = (nt == 256 ? 110 * 1024 : 200 * 1024) - p.S * (p.elem + sizeof(int));
   const size_t real = p.elem / 2;
   const size_t pitch = ts ? ((p.S + p.S / tS_r1(p.S)) | 1) : (size_t)p.pitch;
-  // persistent layout (compile-time-S kernel, 512 threads): region A =
-  // max(output tile, staging buffer), region B = staging buffer, an even
-  // number of phases; up to 224 KB
-  const int want_persist = p.knob_s1_persist >= 0 ? p.knob_s1_persist : env_int("SOI_STAGE1_PERSIST", 1);
-  if (ts && nt == 512 && want_persist) {
-    const size_t pbudget = 224 * 1024 - p.S * (p.elem + sizeof(int));
-    for (int jt = groups * jr; jt >= jr; jt -= jr) {
-      if ((long long)jt > (long long)p.J - p.atap - jt) continue;
-      for (int ac = p.atap; ac >= 1; --ac) {
-        const int nph = p.dmu * ((p.atap + ac - 1) / ac);
-        if (nph % 2) continue;
-        const size_t rows = (size_t)(jt + ac - 1) * p.S;
-        const size_t fel = ((size_t)ac * p.nmu * p.S * real + p.elem - 1) / p.elem;
-        const size_t be = ((rows + fel) * p.elem + 15) / 16 * 16 / p.elem;
-        const size_t tile = (size_t)p.nmu * jt * pitch;
-        const size_t ba = (std::max(tile, be) * p.elem + 15) / 16 * 16 / p.elem;
-        if ((ba + be) * p.elem <= pbudget) {
-          p.JR2 = jr; p.JT2 = jt; p.AC = ac; p.buf_elems = (int)be; p.bufA_elems = (int)ba;
-          p.smem1b = (ba + be) * p.elem + p.S * (p.elem + sizeof(int));
-          p.s1fast = 1; p.s1_tS = 1; p.s1_nt = 512; p.s1_persist = 1;
-          return;
-        }
-      }
-    }
-  }
   for (int jt = groups * jr; jt >= jr; jt -= jr) {
     if ((long long)jt > (long long)p.J - p.atap - jt) continue;     // keep the wrap single-step
     for (int ac = p.atap; ac >= 1; --ac) {
@@ -801,13 +769,6 @@ int make_plan(const soi_desc_t *d, size_t k, int knob_s1_nt, int knob_s2, bool w
   if (ce != cudaSuccess) { delete p; return SOI_ERR_CUDA; }
   rc = p->prec == SOI_PRECISION_FP64 ? build_tables<double>(*p) : build_tables<float>(*p);
   if (rc) { free_plan(p); return rc; }
-  if (p->s1_persist) {
-    // one CTA per SM (the layout takes more than half of an SM's shared memory)
-    if (cudaDeviceGetAttribute(&p->s1_grid, cudaDevAttrMultiProcessorCount, p->device) != cudaSuccess) {
-      free_plan(p);
-      return SOI_ERR_CUDA;
-    }
-  }
   if ((rc = upload_regtw())) { free_plan(p); return rc; }
   if (p->fast2 == 4) {
     p->fast2 = 0;

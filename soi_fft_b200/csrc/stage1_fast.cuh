@@ -29,7 +29,6 @@ struct Conv2Args {
   int S, d, atap, JT, pitch, AC;
   int buf_elems;         // complex elements per staging buffer (rows + filter, rounded)
   int seg_lo, seg_hi;    // segments sigma stored (all: 0, S)
-  int bufA_elems;        // persistent stage 1: complex elements of region A (tile or staging)
 };
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
@@ -206,18 +205,12 @@ template <typename V> struct EmitTransposed {
 
 // Same kernel with the segment count S = R0*R1 and the block size NT known at
 // compile time (NT = 256 runs two CTAs per SM, so one CTA's convolution
-// overlaps the other's FFT and stores): shared addressing becomes immediate
-// offsets, and the S-point FFT runs as two register-radix stages (RegDFT)
-// whose last stage writes the transposed output straight to HBM.  Tile
-// layout: row r, column s at r*PITCH + s + s/R1, PITCH odd.
-//
-// PERSIST: one CTA per SM walks the tiles blockIdx.x, + gridDim.x, ...  Shared
-// memory is region A (the output tile, or a staging buffer) and region B (a
-// staging buffer).  Phase p of a tile is staged in B when nphase - 1 - p is
-// odd, else in A, so the last phase lands in A (nphase is even) and B is free
-// during the last phase: the next tile's first phase is copied into B while
-// this tile finishes its convolution, its S-point FFT and its stores.
-template <typename R, int NMU, int JR, int R0, int R1, int NT, bool PERSIST>
+// overlaps the other's FFT and stores): shared
+// addressing becomes immediate offsets, and the S-point FFT runs as two
+// register-radix stages (RegDFT) whose last stage writes the transposed
+// output straight to HBM.  Tile layout: row r, column s at
+// r*PITCH + s + s/R1, PITCH odd.
+template <typename R, int NMU, int JR, int R0, int R1, int NT>
 __global__ void __launch_bounds__(NT, 512 / NT) k_conv_sfft_tS(Conv2Args a)
 {
   using V = typename cplx_of<R>::type;
@@ -226,32 +219,26 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_conv_sfft_tS(Conv2Args a)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int JT = a.JT;
   const int rows_tile = NMU * JT;
-  V *regA = reinterpret_cast<V *>(smem_raw);
-  V *regB = regA + (PERSIST ? a.bufA_elems : a.buf_elems);
-  V *tile = regA;
-  V *twS = regB + a.buf_elems;
+  V *buf0 = reinterpret_cast<V *>(smem_raw);
+  V *buf1 = buf0 + a.buf_elems;
+  V *tile = buf0;
+  V *twS = buf0 + 2 * (size_t)a.buf_elems;
   const int tid = threadIdx.x;
   for (int i = tid; i < S; i += blockDim.x) twS[i] = reinterpret_cast<const V *>(a.twS)[i];
   const int s = tid % S;
   const int jb = tid / S;
   const bool active = jb * JR < JT;
+  const long long j0 = (long long)blockIdx.x * JT;
   const int d = a.d;
   const long long M = a.M;
   const int nch = (a.atap + a.AC - 1) / a.AC;
   const int nphase = d * nch;
-  const long long ntiles = (a.J + JT - 1) / JT;
   const V *alpha = reinterpret_cast<const V *>(a.alpha);
   const R *filt = reinterpret_cast<const R *>(a.filt);
   constexpr int CPR = S * (int)sizeof(V) / 16;                // 16-byte chunks per input row
   static_assert(NT % CPR == 0, "row chunks must tile the block");
 
-  auto bufp = [&](int p) -> V * {
-    if (PERSIST) return ((nphase - 1 - p) & 1) ? regB : regA;
-    return (p & 1) ? regB : regA;
-  };
-  // copy phase p (branch b = p / nch, taps [a_lo, a_lo + n_a)) of the tile
-  // starting at output group j0 into dst
-  auto issue = [&](long long j0, int p, V *dst) {
+  auto issue = [&](int p, V *dst) {
     const int b = p / nch, a_lo = (p % nch) * a.AC;
     const int n_a = min(a.AC, a.atap - a_lo);
     const int nrows = JT + n_a - 1;
@@ -268,98 +255,80 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_conv_sfft_tS(Conv2Args a)
     for (int c = tid; c < fchunks; c += NT) cp_async16(reinterpret_cast<char *>(fdst) + c * 16, fsrc + c * 16);
   };
 
-  long long tl = blockIdx.x;
-  if (tl >= ntiles) return;
-  issue(tl * JT, 0, bufp(0));
-  cp_async_commit();
-  for (;;) {
-    const long long j0 = tl * JT;
-    const long long next = PERSIST ? tl + gridDim.x : ntiles;
-    V acc[JR][NMU];
+  V acc[JR][NMU];
 #pragma unroll
-    for (int jj = 0; jj < JR; ++jj)
+  for (int jj = 0; jj < JR; ++jj)
 #pragma unroll
-      for (int th = 0; th < NMU; ++th) acc[jj][th] = cmk<V>((R)0, (R)0);
+    for (int th = 0; th < NMU; ++th) acc[jj][th] = cmk<V>((R)0, (R)0);
 
-    for (int p = 0; p < nphase; ++p) {
-      const V *cur = bufp(p);
-      bool issued = false;
-      if (p + 1 < nphase) {
-        issue(j0, p + 1, bufp(p + 1));
-        issued = true;
-      } else if (PERSIST && next < ntiles) {
-        issue(next * JT, 0, bufp(0));                        // B: free since phase nphase - 2
-        issued = true;
-      }
-      if (issued) {
-        cp_async_commit();
-        cp_async_wait<1>();
-      } else {
-        cp_async_wait<0>();
-      }
-      __syncthreads();
-      if (active) {
-        const int a_lo = (p % nch) * a.AC;
-        const int n_a = min(a.AC, a.atap - a_lo);
-        const int nrows = JT + n_a - 1;
-        const V *rows = cur + (size_t)(jb * JR) * S + s;        // rows[t*S] = x_b[j0 + a_lo + jb*JR + t]
-        const R *fb = reinterpret_cast<const R *>(cur + (size_t)nrows * S) + s;   // fb[(u*NMU + th)*S]
-        V xw[JR];
-#pragma unroll
-        for (int jj = 0; jj < JR - 1; ++jj) xw[jj] = rows[jj * S];
-        const int nmain = n_a - n_a % JR;
-        for (int u0 = 0; u0 < nmain; u0 += JR) {
-          const V *rp = rows + (size_t)u0 * S;
-          const R *fp = fb + (size_t)u0 * NMU * S;
-#pragma unroll
-          for (int u = 0; u < JR; ++u) {
-            xw[(u + JR - 1) % JR] = rp[(u + JR - 1) * S];
-            R h[NMU];
-#pragma unroll
-            for (int th = 0; th < NMU; ++th) h[th] = fp[(u * NMU + th) * S];
-#pragma unroll
-            for (int jj = 0; jj < JR; ++jj)
-#pragma unroll
-              for (int th = 0; th < NMU; ++th) macc(acc[jj][th], h[th], xw[(u + jj) % JR]);
-          }
-        }
-        const V *rp = rows + (size_t)nmain * S;
-        const R *fp = fb + (size_t)nmain * NMU * S;
-#pragma unroll
-        for (int u = 0; u < JR - 1; ++u) {
-          if (u < n_a - nmain) {
-            xw[(u + JR - 1) % JR] = rp[(u + JR - 1) * S];
-            R h[NMU];
-#pragma unroll
-            for (int th = 0; th < NMU; ++th) h[th] = fp[(u * NMU + th) * S];
-#pragma unroll
-            for (int jj = 0; jj < JR; ++jj)
-#pragma unroll
-              for (int th = 0; th < NMU; ++th) macc(acc[jj][th], h[th], xw[(u + jj) % JR]);
-          }
-        }
-      }
-      __syncthreads();
+  issue(0, buf0);
+  cp_async_commit();
+  for (int p = 0; p < nphase; ++p) {
+    V *cur = (p & 1) ? buf1 : buf0;
+    if (p + 1 < nphase) {
+      issue(p + 1, (p & 1) ? buf0 : buf1);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
-    // epilogue: the tile takes region A (its last phase is consumed); with
-    // PERSIST the next tile's first phase is arriving in B meanwhile
+    __syncthreads();
     if (active) {
-      const V *ph = reinterpret_cast<const V *>(a.phase);
+      const int a_lo = (p % nch) * a.AC;
+      const int n_a = min(a.AC, a.atap - a_lo);
+      const int nrows = JT + n_a - 1;
+      const V *rows = cur + (size_t)(jb * JR) * S + s;        // rows[t*S] = x_b[j0 + a_lo + jb*JR + t]
+      const R *fb = reinterpret_cast<const R *>(cur + (size_t)nrows * S) + s;   // fb[(u*NMU + th)*S]
+      V xw[JR];
 #pragma unroll
-      for (int th = 0; th < NMU; ++th) {
-        const V pz = __ldg(ph + th * S + s);
+      for (int jj = 0; jj < JR - 1; ++jj) xw[jj] = rows[jj * S];
+      const int nmain = n_a - n_a % JR;
+      for (int u0 = 0; u0 < nmain; u0 += JR) {
+        const V *rp = rows + (size_t)u0 * S;
+        const R *fp = fb + (size_t)u0 * NMU * S;
 #pragma unroll
-        for (int jj = 0; jj < JR; ++jj)
-          tile[(size_t)((jb * JR + jj) * NMU + th) * PITCH + s + s / R1] = cmul(pz, acc[jj][th]);
+        for (int u = 0; u < JR; ++u) {
+          xw[(u + JR - 1) % JR] = rp[(u + JR - 1) * S];
+          R h[NMU];
+#pragma unroll
+          for (int th = 0; th < NMU; ++th) h[th] = fp[(u * NMU + th) * S];
+#pragma unroll
+          for (int jj = 0; jj < JR; ++jj)
+#pragma unroll
+            for (int th = 0; th < NMU; ++th) macc(acc[jj][th], h[th], xw[(u + jj) % JR]);
+        }
+      }
+      const V *rp = rows + (size_t)nmain * S;
+      const R *fp = fb + (size_t)nmain * NMU * S;
+#pragma unroll
+      for (int u = 0; u < JR - 1; ++u) {
+        if (u < n_a - nmain) {
+          xw[(u + JR - 1) % JR] = rp[(u + JR - 1) * S];
+          R h[NMU];
+#pragma unroll
+          for (int th = 0; th < NMU; ++th) h[th] = fp[(u * NMU + th) * S];
+#pragma unroll
+          for (int jj = 0; jj < JR; ++jj)
+#pragma unroll
+            for (int th = 0; th < NMU; ++th) macc(acc[jj][th], h[th], xw[(u + jj) % JR]);
+        }
       }
     }
     __syncthreads();
-    EmitTransposed<V> e{ reinterpret_cast<V *>(a.T), a.Mh, (long long)NMU * j0, a.seg_lo, a.seg_hi };
-    tile_fft_smem<V, R0, R1, 1>(tile, rows_tile, 1, PITCH, twS, e);
-    if (!PERSIST || next >= ntiles) break;
-    __syncthreads();                                          // region A is read by the FFT's last stage
-    tl = next;
   }
+  if (active) {
+    const V *ph = reinterpret_cast<const V *>(a.phase);
+#pragma unroll
+    for (int th = 0; th < NMU; ++th) {
+      const V pz = __ldg(ph + th * S + s);
+#pragma unroll
+      for (int jj = 0; jj < JR; ++jj)
+        tile[(size_t)((jb * JR + jj) * NMU + th) * PITCH + s + s / R1] = cmul(pz, acc[jj][th]);
+    }
+  }
+  __syncthreads();
+  EmitTransposed<V> e{ reinterpret_cast<V *>(a.T), a.Mh, (long long)NMU * j0, a.seg_lo, a.seg_hi };
+  tile_fft_smem<V, R0, R1, 1>(tile, rows_tile, 1, PITCH, twS, e);
 }
 
 }  // namespace soi

@@ -90,24 +90,34 @@ __device__ __forceinline__ void tile_fft_smem(V *sm, int C, int PP, int PC, cons
   constexpr int L = R0 * R1 * R2;
   constexpr int span0 = L / R0;
   auto sidx = [&](int col, int pos) { return (pos + pos / RL) * PP + col * PC; };
+  // item q = i*C + col; (col, i) advance by the block size without dividing
+  const int nt = blockDim.x, dcol = nt % C, di = nt / C;
   {
     const int n = C * span0;
-    for (int q = threadIdx.x; q < n; q += blockDim.x) {
-      const int col = q % C, i = q / C;
+    int col = threadIdx.x % C, i = threadIdx.x / C;
+    // the R0 values of a butterfly sit at one base plus multiples of the
+    // shared distance of span0 positions (span0 is a whole number of pad groups)
+    static_assert(span0 % RL == 0, "first-stage stride is a whole number of pad groups");
+    const int D0 = (span0 + span0 / RL) * PP;
+    for (int q = threadIdx.x; q < n; q += nt, col += dcol, i += di) {
+      if (col >= C) { col -= C; ++i; }
+      V *p = sm + sidx(col, i);
       V v[R0];
 #pragma unroll
-      for (int r = 0; r < R0; ++r) v[r] = sm[sidx(col, i + r * span0)];
+      for (int r = 0; r < R0; ++r) v[r] = p[r * D0];
       RegDFT<V, R0>::run(v);
+      p[0] = v[0];
 #pragma unroll
-      for (int k = 0; k < R0; ++k) sm[sidx(col, i + k * span0)] = (k && i) ? cmul(v[k], tw[i * k]) : v[k];
+      for (int k = 1; k < R0; ++k) p[k * D0] = cmul(v[k], tw[i * k]);     // tw[0] = 1 exactly
     }
   }
   __syncthreads();
   if constexpr (R2 > 1) {
     constexpr int span1 = span0 / R1;
     const int n = C * (L / R1);
-    for (int q = threadIdx.x; q < n; q += blockDim.x) {
-      const int col = q % C, t = q / C;
+    int col = threadIdx.x % C, t = threadIdx.x / C;
+    for (int q = threadIdx.x; q < n; q += nt, col += dcol, t += di) {
+      if (col >= C) { col -= C; ++t; }
       const int blk = t / span1, i = t - blk * span1;
       const int base = blk * span0 + i;
       V v[R1];
@@ -121,11 +131,13 @@ __device__ __forceinline__ void tile_fft_smem(V *sm, int C, int PP, int PC, cons
   }
   {
     const int n = C * (L / RL);
-    for (int q = threadIdx.x; q < n; q += blockDim.x) {
-      const int col = q % C, blk = q / C;
+    int col = threadIdx.x % C, blk = threadIdx.x / C;
+    for (int q = threadIdx.x; q < n; q += nt, col += dcol, blk += di) {
+      if (col >= C) { col -= C; ++blk; }
+      const V *p = sm + blk * (RL + 1) * PP + col * PC;
       V v[RL];
 #pragma unroll
-      for (int r = 0; r < RL; ++r) v[r] = sm[sidx(col, blk * RL + r)];
+      for (int r = 0; r < RL; ++r) v[r] = p[r * PP];
       RegDFT<V, RL>::run(v);
       int fbase;
       if constexpr (R2 > 1) fbase = (blk / R1) + R0 * (blk % R1);

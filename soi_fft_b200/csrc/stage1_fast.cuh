@@ -189,15 +189,22 @@ struct NoPrep {};
 
 template <typename V> struct EmitTransposed {
   V *T; long long Mh, rho0; int lo, hi;   // segments f in [lo, hi) are stored
+  bool all;                                // [lo, hi) covers every segment
   __device__ __forceinline__ NoPrep prepare(int, int) const { return NoPrep{}; }
   template <int RL> __device__ __forceinline__ void run(int col, int fbase, int fstep, V *v, NoPrep = NoPrep{}) const
   {
     const long long rho = rho0 + col;
     if (rho < Mh) {
+      V *dst = T + (size_t)fbase * Mh + rho;
+      if (all) {
 #pragma unroll
-      for (int k = 0; k < RL; ++k) {
-        const int f = fbase + fstep * k;
-        if (f >= lo && f < hi) T[(size_t)f * Mh + rho] = v[k];
+        for (int k = 0; k < RL; ++k) dst[(size_t)k * fstep * Mh] = v[k];
+      } else {
+#pragma unroll
+        for (int k = 0; k < RL; ++k) {
+          const int f = fbase + fstep * k;
+          if (f >= lo && f < hi) dst[(size_t)k * fstep * Mh] = v[k];
+        }
       }
     }
   }
@@ -238,21 +245,33 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_conv_sfft_tS(Conv2Args a)
   constexpr int CPR = S * (int)sizeof(V) / 16;                // 16-byte chunks per input row
   static_assert(NT % CPR == 0, "row chunks must tile the block");
 
+  // copy phase p (branch b = p / nch, taps [a_lo, a_lo + n_a)) into dst:
+  // input row t of the phase is x_b[j0 + a_lo + t] = alpha row d*(j0 + a_lo + t) + b,
+  // read circularly (the ghost rows of .cpp:495-515); each thread steps its
+  // source and destination pointers by NT/CPR rows
+  constexpr size_t ROWB = (size_t)S * sizeof(V);
+  const char *alpha_end = reinterpret_cast<const char *>(alpha) + (size_t)M * ROWB;
   auto issue = [&](int p, V *dst) {
     const int b = p / nch, a_lo = (p % nch) * a.AC;
     const int n_a = min(a.AC, a.atap - a_lo);
     const int nrows = JT + n_a - 1;
     const int off = tid % CPR;
-    for (int t = tid / CPR; t < nrows; t += NT / CPR) {
-      long long r = (long long)d * (j0 + a_lo + t) + b;
-      if (r >= M) r -= M;                                    // circular (ghost rows, .cpp:495-515)
-      cp_async16(reinterpret_cast<char *>(dst + (size_t)t * S) + off * 16,
-                 reinterpret_cast<const char *>(alpha + r * S) + off * 16);
+    int t = tid / CPR;
+    long long r = (long long)d * (j0 + a_lo + t) + b;
+    if (r >= M) r -= M;
+    const char *src = reinterpret_cast<const char *>(alpha) + (size_t)r * ROWB + off * 16;
+    char *dp = reinterpret_cast<char *>(dst) + (size_t)t * ROWB + off * 16;
+    const size_t dsrc = (size_t)d * (NT / CPR) * ROWB;
+    for (; t < nrows; t += NT / CPR) {
+      cp_async16(dp, src);
+      dp += (NT / CPR) * ROWB;
+      src += dsrc;
+      if (src >= alpha_end) src -= (size_t)M * ROWB;          // the wrap happens at most once per tile
     }
-    R *fdst = reinterpret_cast<R *>(dst + (size_t)nrows * S);
-    const char *fsrc = reinterpret_cast<const char *>(filt + ((size_t)(b * a.atap + a_lo) * NMU) * S);
+    const char *fs = reinterpret_cast<const char *>(filt + ((size_t)(b * a.atap + a_lo) * NMU) * S) + tid * 16;
+    char *fd = reinterpret_cast<char *>(dst + (size_t)nrows * S) + tid * 16;
     const int fchunks = n_a * NMU * S * (int)sizeof(R) / 16;
-    for (int c = tid; c < fchunks; c += NT) cp_async16(reinterpret_cast<char *>(fdst) + c * 16, fsrc + c * 16);
+    for (int c = tid; c < fchunks; c += NT, fs += NT * 16, fd += NT * 16) cp_async16(fd, fs);
   };
 
   V acc[JR][NMU];
@@ -327,7 +346,8 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_conv_sfft_tS(Conv2Args a)
     }
   }
   __syncthreads();
-  EmitTransposed<V> e{ reinterpret_cast<V *>(a.T), a.Mh, (long long)NMU * j0, a.seg_lo, a.seg_hi };
+  EmitTransposed<V> e{ reinterpret_cast<V *>(a.T), a.Mh, (long long)NMU * j0, a.seg_lo, a.seg_hi,
+                      a.seg_lo == 0 && a.seg_hi >= S };
   tile_fft_smem<V, R0, R1, 1>(tile, rows_tile, 1, PITCH, twS, e);
 }
 

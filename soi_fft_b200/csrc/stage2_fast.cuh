@@ -201,37 +201,44 @@ __global__ void __launch_bounds__(NT, 2) k_stage2_ct(S2ArgsCT a)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   V *buf = reinterpret_cast<V *>(smem_raw);
   __shared__ V s_tab[G::TAB];
-  __shared__ unsigned int s_task;
-  __shared__ int s_ok;
+  __shared__ unsigned int s_task[2];
+  __shared__ int s_ok[2];
   const int tid = threadIdx.x;
   const unsigned int total = (unsigned int)a.S * G::PER;
   unsigned int next = 0;
-  if (tid == 0) next = atomicAdd(a.counter, 1u);
-
-  for (;;) {
-    if (tid == 0) {
-      unsigned int t = next;
-      if (t < total) next = atomicAdd(a.counter, 1u);       // claim the following task now
-      if (*(volatile int *)a.err) t = total;
-      int ok = 1;
-      if (t < total && t >= (unsigned int)G::NT1) {
-        const unsigned int u = t - G::NT1;
-        const int blk = (int)(u / G::PER), r = (int)(u % G::PER);
-        if (blk >= a.S - 1 || r >= G::NT1) {                // pass-2 task of segment blk
-          long long it = 0;
-          while (ld_acquire_u32(a.done1 + blk) < (unsigned int)(G::NT1 + a.wait_extra)) {
-            if (++it > kWaitLimit) { atomicExch(a.err, 1); ok = 0; break; }
-            if (*(volatile int *)a.err) { ok = 0; break; }   // another CTA gave up
-            __nanosleep(128);
-          }
+  // thread 0: take the claimed task, claim the one after it, and for a
+  // pass-2 task wait (bounded) until its segment's pass 1 is complete; the
+  // result goes to slot `slot`, read by all threads after the next barrier
+  auto take = [&](int slot) {
+    unsigned int t = next;
+    if (t < total) next = atomicAdd(a.counter, 1u);
+    if (*(volatile int *)a.err) t = total;
+    int ok = 1;
+    if (t < total && t >= (unsigned int)G::NT1) {
+      const unsigned int u = t - G::NT1;
+      const int blk = (int)(u / G::PER), r = (int)(u % G::PER);
+      if (blk >= a.S - 1 || r >= G::NT1) {                  // pass-2 task of segment blk
+        long long it = 0;
+        while (ld_acquire_u32(a.done1 + blk) < (unsigned int)(G::NT1 + a.wait_extra)) {
+          if (++it > kWaitLimit) { atomicExch(a.err, 1); ok = 0; break; }
+          if (*(volatile int *)a.err) { ok = 0; break; }   // another CTA gave up
+          __nanosleep(128);
         }
       }
-      s_task = t;
-      s_ok = ok;
     }
-    __syncthreads();
-    const unsigned int t = s_task;
-    if (t >= total || !s_ok) break;
+    s_task[slot] = t;
+    s_ok[slot] = ok;
+  };
+  if (tid == 0) {
+    next = atomicAdd(a.counter, 1u);
+    take(0);
+  }
+  __syncthreads();
+
+  for (int iter = 0;; ++iter) {
+    const int slot = iter & 1;
+    const unsigned int t = s_task[slot];
+    if (t >= total || !s_ok[slot]) break;
     int kind, seg, tile;
     if (t < (unsigned int)G::NT1) { kind = 1; seg = 0; tile = (int)t; }
     else {
@@ -258,10 +265,11 @@ __global__ void __launch_bounds__(NT, 2) k_stage2_ct(S2ArgsCT a)
       __syncthreads();
       EmitColsCT<V, C, M2, RLA> e{ Tseg, m2_0, s_tab, &a };
       tile_fft_ct<V, A0, A1, A2, C, C, 1, NT>(buf, reinterpret_cast<const V *>(a.tw1), e);
-      __syncthreads();
+      __syncthreads();                                        // every store of the tile is issued
       if (tid == 0) {
         __threadfence();
-        atomicAdd(a.done1 + seg, 1u);
+        atomicAdd(a.done1 + seg, 1u);                         // publish, then take the next task
+        take(slot ^ 1);
       }
     } else {
       const int k1_0 = tile * C;
@@ -289,8 +297,9 @@ __global__ void __launch_bounds__(NT, 2) k_stage2_ct(S2ArgsCT a)
       }
       EmitRowsCT<V, M1, RLB> e{ reinterpret_cast<V *>(a.out) + (size_t)(a.seg_lo + seg) * a.M, k1_0, s_tab, &a };
       tile_fft_ct<V, B0, B1, B2, C, 1, G::PS2, NT>(buf, reinterpret_cast<const V *>(a.tw2), e);
+      if (tid == 0) take(slot ^ 1);                           // after thread 0's own stores
     }
-    __syncthreads();
+    __syncthreads();                                          // the tile buffer is free, the next task is known
   }
 }
 

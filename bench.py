@@ -205,6 +205,8 @@ class ClockSampler:
 
 
 def dist_setup(args):
+    """One process per GPU (torchrun's RANK/LOCAL_RANK/WORLD_SIZE); NCCL for
+    the barrier and the max-over-ranks time, gloo where there is no GPU."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -213,10 +215,28 @@ def dist_setup(args):
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        backend = "gloo"
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            backend = "nccl"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
         pg = dist
     return world, rank, local, pg
+
+
+def max_over_ranks(pg, v, device=None):
+    """The largest of the ranks' values (the job's time is its slowest rank's)."""
+    if not pg:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(world, flop_per_step, steps, ms):
+    """Whole-job throughput: every rank's steps over the slowest rank's time."""
+    return world * flop_per_step * steps / (ms / 1e3) / 1e9
 
 
 def make_signal(N, seed, device):
@@ -266,7 +286,9 @@ def cpu_baseline(log2n, S, steps, threads=None, bounded=True):
 # ------------------------------------------------------------- reference ---
 
 def run_reference(args):
-    world, rank, _, pg = dist_setup(args)
+    # the reference's CPU path runs once, on rank 0; other ranks exit without
+    # work (no process group is needed)
+    rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     log2n = min(args.log2n, CPU_SAMPLE_LOG2N)
@@ -315,12 +337,8 @@ def run_ours(args):
             pg.barrier()
         torch.cuda.synchronize(dev)
 
-    def max_over_ranks(v):
-        if not pg:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
+    def max_over_ranks_(v):
+        return max_over_ranks(pg, v, dev)
 
     def timed(d, src, dst, steps, warmup, per_stage=False):
         for _ in range(warmup):
@@ -349,7 +367,7 @@ def run_ours(args):
     with ClockSampler(local) as clk:
         ms, _ = timed(d32, x32, y32, args.steps, args.warmup)
     clocks = clk.summary()
-    ms = max_over_ranks(ms)
+    ms = max_over_ranks_(ms)
     ms_step = ms / args.steps
     value = world * flop(N) * args.steps / (ms / 1e3) / 1e9
 
@@ -383,14 +401,14 @@ def run_ours(args):
     d32.compute_stream([hi] * e2e_steps, [ho] * e2e_steps)
     e1.record(stream)
     barrier()
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps)
+    e2e_ms = max_over_ranks_(e0.elapsed_time(e1) / e2e_steps)
     e2e_value = world * flop(N) / (e2e_ms / 1e3) / 1e9
     e0.record(stream)
     for _ in range(2):
         d32.compute_into(hi, ho)
     e1.record(stream)
     barrier()
-    single_ms = max_over_ranks(e0.elapsed_time(e1) / 2)
+    single_ms = max_over_ranks_(e0.elapsed_time(e1) / 2)
     d32.free()
     del h_in, h_out
 
@@ -400,7 +418,7 @@ def run_ours(args):
         d64 = new_desc(sb.PRECISION_FP64)
         y64 = torch.empty_like(x128)
         ms64, _ = timed(d64, x128, y64, max(2, min(args.steps, 5)), 2)
-        ms64 = max_over_ranks(ms64) / max(2, min(args.steps, 5))
+        ms64 = max_over_ranks_(ms64) / max(2, min(args.steps, 5))
         acc64 = float(torch.linalg.norm(y64 - X) / nX)
         fp64 = {"value": world * flop(N) / (ms64 / 1e3) / 1e9, "unit": "GFLOP/s", "ms_per_step": ms64,
                 "rel_l2_vs_fp64_direct_fft": acc64}
@@ -514,11 +532,7 @@ def run_batched(args):
         e1.synchronize()
     b.check()
     clocks = clk.summary()
-    ms = e0.elapsed_time(e1)
-    if pg:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(pg, e0.elapsed_time(e1), dev)
     nominal = sum(flop(w["N"]) for w in wl)
     band_frac = sum((w["seg_hi"] - w["seg_lo"]) / w["k"] * w["N"] for w in wl) / sum(w["N"] for w in wl)
     if rank == 0:

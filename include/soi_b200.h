@@ -95,6 +95,8 @@ void free_soi_descriptor(soi_desc_t *desc);
 void parallel_filter_subsampling(soi_desc_t *desc, void *alpha_dt);
 
 /* ---- status-returning variants ---------------------------------------- */
+/* Device inputs (device_ptr = 1) must start on a 16-byte boundary (memory
+ * from cudaMalloc does); a misaligned input returns SOI_ERR_INVALID. */
 int soi_init_status(soi_desc_t *desc, soi_comm_t comm, cfft_size_t k);
 int soi_compute_status(soi_desc_t *desc, void *alpha_dt);
 /* Out-of-place compute_soi: `in` (N inputs) is left untouched, `out`

@@ -69,11 +69,13 @@ struct Plan {
   int s1fast = 0, JR2 = 0, JT2 = 0, AC = 0, buf_elems = 0;
   int s1_tS = 0;                    // compile-time-S stage-1 instance available
   int s1_nt = 512;                  // its block size (256: two CTAs per SM)
+  int s1_bulk = 0;                  // its staging by bulk copies (512 threads)
   size_t smem1b = 0;
   void *d_filt2 = nullptr;          // [d][atap][nmu][S] real
   // variant choices forced by the batch tuner (-1: defaults / SOI_* switches)
   int knob_s1_nt = -1;              // 256 or 512 threads for the compile-time-S stage 1
   int knob_s2 = -1;                 // 1 persistent stage 2, 0 two-kernel stage 2
+  int knob_s1_bulk = -1;            // 1/0: stage-1 staging by bulk copies or cp.async
   bool timing = false;
   cudaEvent_t ev[5] = {};
   float ms[4] = {0, 0, 0, 0};
@@ -402,7 +404,6 @@ int setup_s2ct(Plan &p, int idx)
   CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, p.device));
   if (occ < 1) return SOI_ERR_UNSUPPORTED;
   p.f2_grid = occ * nsm;
-  CK(cudaMalloc(&p.d_sync, (p.S + 2) * sizeof(unsigned int)));
   int rc = p.prec == SOI_PRECISION_FP64 ? build_demod_tables<double>(p, true) : build_demod_tables<float>(p, true);
   if (rc) return rc;
   p.discard = env_int("SOI_STAGE2_DISCARD", 1);
@@ -431,11 +432,12 @@ int launch_s2ct(Plan &p, const Exec &ex)
   return SOI_OK;
 }
 
-// Error flag of the persistent stage-2 kernel (a dependency wait that gave
-// up); synchronises the stream.
+// Error word of an execution (a stage-1 staging wait or a stage-2
+// dependency wait that gave up); synchronises the stream.
 int check_stage2(Plan &p, const unsigned int *sync, cudaStream_t st)
 {
-  if (!p.fast2 || !sync) return SOI_OK;
+  (void)p;
+  if (!sync) return SOI_OK;
   int err = 0;
   CK(cudaMemcpyAsync(&err, sync, sizeof(int), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
@@ -466,7 +468,7 @@ int staged_jr(int prec, int nmu)
   return nmu == 5 ? 4 : nmu == 3 ? 4 : (nmu == 8 || nmu == 9) ? 2 : 0;
 }
 
-template <typename R, int NMU, int JR, int R0, int R1, int NT>
+template <typename R, int NMU, int JR, int R0, int R1, int NT, bool BULK>
 int launch_conv_tS(Plan &p, const Exec &ex)
 {
   Conv2Args a;
@@ -475,7 +477,8 @@ int launch_conv_tS(Plan &p, const Exec &ex)
   a.M = (long long)p.M; a.Mh = (long long)p.Mh; a.J = (long long)p.J;
   a.S = (int)p.S; a.d = p.dmu; a.atap = p.atap; a.JT = p.JT2; a.pitch = p.pitch; a.AC = p.AC;
   a.buf_elems = p.buf_elems;
-  auto kern = k_conv_sfft_tS<R, NMU, JR, R0, R1, NT>;
+  a.err = (int *)ex.sync;
+  auto kern = k_conv_sfft_tS<R, NMU, JR, R0, R1, NT, BULK>;
   CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem1b));
   dim3 grid((unsigned)((p.J + p.JT2 - 1) / p.JT2));
   kern<<<grid, NT, p.smem1b, ex.st>>>(a);
@@ -484,16 +487,16 @@ int launch_conv_tS(Plan &p, const Exec &ex)
 }
 
 // compile-time-S instances: n_mu = 5, S in {8..256} (R0*R1 split of S)
-template <typename R, int JR, int NT>
+template <typename R, int JR, int NT, bool BULK>
 int launch_tS_switch_nt(Plan &p, const Exec &ex)
 {
   switch (p.S) {
-    case 8: return launch_conv_tS<R, 5, JR, 2, 4, NT>(p, ex);
-    case 16: return launch_conv_tS<R, 5, JR, 4, 4, NT>(p, ex);
-    case 32: return launch_conv_tS<R, 5, JR, 4, 8, NT>(p, ex);
-    case 64: return launch_conv_tS<R, 5, JR, 8, 8, NT>(p, ex);
-    case 128: return launch_conv_tS<R, 5, JR, 8, 16, NT>(p, ex);
-    case 256: return launch_conv_tS<R, 5, JR, 16, 16, NT>(p, ex);
+    case 8: return launch_conv_tS<R, 5, JR, 2, 4, NT, BULK>(p, ex);
+    case 16: return launch_conv_tS<R, 5, JR, 4, 4, NT, BULK>(p, ex);
+    case 32: return launch_conv_tS<R, 5, JR, 4, 8, NT, BULK>(p, ex);
+    case 64: return launch_conv_tS<R, 5, JR, 8, 8, NT, BULK>(p, ex);
+    case 128: return launch_conv_tS<R, 5, JR, 8, 16, NT, BULK>(p, ex);
+    case 256: return launch_conv_tS<R, 5, JR, 16, 16, NT, BULK>(p, ex);
   }
   return SOI_ERR_UNSUPPORTED;
 }
@@ -501,7 +504,8 @@ int launch_tS_switch_nt(Plan &p, const Exec &ex)
 template <typename R, int JR>
 int launch_tS_switch(Plan &p, const Exec &ex)
 {
-  return p.s1_nt == 256 ? launch_tS_switch_nt<R, JR, 256>(p, ex) : launch_tS_switch_nt<R, JR, 512>(p, ex);
+  if (p.s1_nt == 256) return launch_tS_switch_nt<R, JR, 256, false>(p, ex);
+  return p.s1_bulk ? launch_tS_switch_nt<R, JR, 512, true>(p, ex) : launch_tS_switch_nt<R, JR, 512, false>(p, ex);
 }
 
 bool tS_available(const Plan &p)
@@ -570,6 +574,7 @@ void plan_stage1_staged(Plan &p)
         p.s1fast = 1;
         p.s1_tS = ts ? 1 : 0;
         p.s1_nt = ts ? nt : 512;
+        p.s1_bulk = ts && nt == 512 && (p.knob_s1_bulk >= 0 ? p.knob_s1_bulk : env_int("SOI_STAGE1_BULK", 1)) ? 1 : 0;
         return;
       }
     }
@@ -770,6 +775,12 @@ int make_plan(const soi_desc_t *d, size_t k, int knob_s1_nt, int knob_s2, bool w
   rc = p->prec == SOI_PRECISION_FP64 ? build_tables<double>(*p) : build_tables<float>(*p);
   if (rc) { free_plan(p); return rc; }
   if ((rc = upload_regtw())) { free_plan(p); return rc; }
+  // error word and stage-2 counters: [0] error flag, [1] task counter, [2 .. 2 + S) pass-1 counts
+  if (cudaMalloc(&p->d_sync, (p->S + 2) * sizeof(unsigned int)) != cudaSuccess ||
+      cudaMemset(p->d_sync, 0, (p->S + 2) * sizeof(unsigned int)) != cudaSuccess) {
+    free_plan(p);
+    return SOI_ERR_CUDA;
+  }
   if (p->fast2 == 4) {
     p->fast2 = 0;
     if ((rc = setup_s2ct(*p, p->f2_variant))) { free_plan(p); return rc; }
@@ -816,6 +827,9 @@ int compute_impl(soi_desc_t *d, const void *in, void *out, bool stage1_only, int
   if (seg_hi < 0) seg_hi = (int)p->S;
   if (seg_lo < 0 || seg_hi > (int)p->S || seg_lo >= seg_hi) return SOI_ERR_INVALID;
   if (!sync_after && !d->device_ptr) return SOI_ERR_INVALID;     // host buffers need the copies to finish
+  // stage 1 stages its input rows with 16-byte copies: a device input must
+  // start on a 16-byte boundary (host inputs go through an aligned buffer)
+  if (d->device_ptr && ((uintptr_t)in & 15)) return SOI_ERR_INVALID;
   if (cudaSetDevice(p->device) != cudaSuccess) return SOI_ERR_CUDA;
   cudaStream_t st = p->stream;
   const size_t bytes = p->N * p->elem;
@@ -829,14 +843,14 @@ int compute_impl(soi_desc_t *d, const void *in, void *out, bool stage1_only, int
   }
   int rc;
   const Exec ex{ src, p->d_T, dst, p->d_sync, seg_lo, seg_hi, st };
-  if (p->fast2) CK(cudaMemsetAsync(p->d_sync, 0, sizeof(unsigned int), st));   // error flag
+  CK(cudaMemsetAsync(p->d_sync, 0, sizeof(unsigned int), st));   // error flag
   if (p->timing) CK(cudaEventRecord(p->ev[0], st));
   if ((rc = run_stage1(*p, ex))) return rc;
   if (p->timing) CK(cudaEventRecord(p->ev[1], st));
   if (stage1_only) {
     if (!sync_after) return SOI_OK;
     CK(cudaStreamSynchronize(st));
-    return SOI_OK;
+    return check_stage2(*p, p->d_sync, st);
   }
   if (d->use_vlc && (rc = run_vlc(*p, ex))) return rc;
   if (p->timing) CK(cudaEventRecord(p->ev[2], st));
@@ -1261,7 +1275,7 @@ int compute_stream_impl(soi_desc_t *d, const void *const *ins, void *const *outs
   cudaStream_t st = p->stream;
   void *buf[2] = { p->d_io, p->d_io2 };
   cudaEvent_t *in_done = p->sev, *comp_done = p->sev + 2, *out_done = p->sev + 4;
-  if (p->fast2) CK(cudaMemsetAsync(p->d_sync, 0, sizeof(unsigned int), st));
+  CK(cudaMemsetAsync(p->d_sync, 0, sizeof(unsigned int), st));
   // the copy streams start after everything already queued on the plan's stream
   CK(cudaEventRecord(comp_done[0], st));
   CK(cudaStreamWaitEvent(p->st_in, comp_done[0], 0));
@@ -1329,7 +1343,7 @@ int compute_inverse_impl(soi_desc_t *d, const void *in, void *out)
   }
   int rc;
   if ((rc = conj_scale(*p, in, buf, p->N, 1.0, st))) return rc;
-  if (p->fast2) CK(cudaMemsetAsync(p->d_sync, 0, sizeof(unsigned int), st));
+  CK(cudaMemsetAsync(p->d_sync, 0, sizeof(unsigned int), st));
   const Exec ex{ buf, p->d_T, buf, p->d_sync, 0, (int)p->S, st };
   if ((rc = run_stage1(*p, ex))) return rc;
   if (d->use_vlc && (rc = run_vlc(*p, ex))) return rc;
@@ -1343,6 +1357,7 @@ int compute_inverse_impl(soi_desc_t *d, const void *in, void *out)
 int soi_compute_inverse_status(soi_desc_t *d, const void *in, void *out)
 {
   if (!d) return SOI_ERR_INVALID;
+  if (d->device_ptr && ((uintptr_t)out & 15)) return SOI_ERR_INVALID;   // the conjugated input is staged in out
   int rc = (in && out) ? compute_inverse_impl(d, in, out) : SOI_ERR_INVALID;
   d->last_status = rc;
   return rc;
@@ -1407,6 +1422,7 @@ int soi_filter_subsample_device(soi_desc_t *d, const void *alpha_dev, void *T_de
   Plan *p = plan_of(d);
   if (!p) return SOI_ERR_NOT_INITIALISED;
   if (cudaSetDevice(p->device) != cudaSuccess) return SOI_ERR_CUDA;
+  if ((uintptr_t)alpha_dev & 15) return SOI_ERR_INVALID;
   const Exec ex{ alpha_dev, T_dev, nullptr, p->d_sync, 0, (int)p->S, p->stream };
   return run_stage1(*p, ex);
 }
@@ -1417,7 +1433,7 @@ int soi_segment_fft_demod_device(soi_desc_t *d, void *T_dev, void *out_dev)
   if (!p) return SOI_ERR_NOT_INITIALISED;
   if (cudaSetDevice(p->device) != cudaSuccess) return SOI_ERR_CUDA;
   const Exec ex{ nullptr, T_dev, out_dev, p->d_sync, 0, (int)p->S, p->stream };
-  if (p->fast2) CK(cudaMemsetAsync(p->d_sync, 0, sizeof(unsigned int), p->stream));
+  CK(cudaMemsetAsync(p->d_sync, 0, sizeof(unsigned int), p->stream));
   int rc = run_stage2(*p, ex);
   if (rc == SOI_OK) rc = check_stage2(*p, p->d_sync, p->stream);
   return rc;
@@ -1570,6 +1586,7 @@ int soi_batch_create(soi_batch_t **batch, const soi_desc_t *tmpl, const soi_batc
   for (int i = 0; i < count; ++i) {
     const soi_batch_item_t &x = items[i];
     if (!x.in || !x.out || x.k < 1) { delete b; return SOI_ERR_INVALID; }
+    if ((uintptr_t)x.in & 15) { delete b; return SOI_ERR_INVALID; }   // 16-byte staging copies
     BatchItem it;
     it.N = x.N; it.k = x.k; it.in = x.in; it.out = x.out;
     it.lo = x.seg_hi <= 0 ? 0 : x.seg_lo;

@@ -29,6 +29,7 @@ struct Conv2Args {
   int S, d, atap, JT, pitch, AC;
   int buf_elems;         // complex elements per staging buffer (rows + filter, rounded)
   int seg_lo, seg_hi;    // segments sigma stored (all: 0, S)
+  int *err;              // set to 1 when a staging wait gives up (bulk copies)
 };
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
@@ -38,6 +39,36 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// ---- bulk copies (TMA, untiled) completing on an mbarrier ------------------
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count)
+{
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity)
+{
+  unsigned ok;
+  asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+               : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+  return ok != 0;
+}
+// global -> shared, `bytes` (multiple of 16, both addresses 16-byte aligned)
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, unsigned long long *bar)
+{
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+// orders this thread's earlier generic shared accesses before its later
+// async-proxy (bulk copy) writes to shared memory
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+constexpr long long kBulkWaitLimit = 1ll << 22;
 
 // acc += h * x (real h, complex x)
 __device__ __forceinline__ void macc(float2 &acc, float h, float2 x) { acc = __ffma2_rn(make_float2(h, h), x, acc); }
@@ -217,7 +248,12 @@ template <typename V> struct EmitTransposed {
 // register-radix stages (RegDFT) whose last stage writes the transposed
 // output straight to HBM.  Tile layout: row r, column s at
 // r*PITCH + s + s/R1, PITCH odd.
-template <typename R, int NMU, int JR, int R0, int R1, int NT>
+//
+// BULK: each phase is staged by warp 0 with one bulk copy (TMA, untiled) per
+// input row and one for the filter slice, completing on the buffer's
+// mbarrier; all threads wait on the mbarrier's phase parity (bounded: a wait
+// that gives up sets a.err).  Otherwise every thread issues 16-byte cp.async.
+template <typename R, int NMU, int JR, int R0, int R1, int NT, bool BULK>
 __global__ void __launch_bounds__(NT, 512 / NT) k_conv_sfft_tS(Conv2Args a)
 {
   using V = typename cplx_of<R>::type;
@@ -273,6 +309,43 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_conv_sfft_tS(Conv2Args a)
     const int fchunks = n_a * NMU * S * (int)sizeof(R) / 16;
     for (int c = tid; c < fchunks; c += NT, fs += NT * 16, fd += NT * 16) cp_async16(fd, fs);
   };
+  __shared__ unsigned long long s_mbar[2];
+  // the same phase as bulk copies issued by warp 0 onto the buffer's mbarrier
+  auto issue_bulk = [&](int p, V *dst, unsigned long long *bar) {
+    if (tid >= 32) return;
+    const int b = p / nch, a_lo = (p % nch) * a.AC;
+    const int n_a = min(a.AC, a.atap - a_lo);
+    const int nrows = JT + n_a - 1;
+    const unsigned fbytes = (unsigned)(n_a * NMU * S * (int)sizeof(R));
+    if (tid == 0) mbar_expect_tx(bar, (unsigned)(nrows * ROWB) + fbytes);
+    __syncwarp();
+    fence_proxy_async_smem();
+    for (int t = tid; t < nrows; t += 32) {
+      long long r = (long long)d * (j0 + a_lo + t) + b;
+      if (r >= M) r -= M;                                    // circular (ghost rows, .cpp:495-515)
+      bulk_g2s(dst + (size_t)t * S, alpha + r * S, (unsigned)ROWB, bar);
+    }
+    if (tid == 31)
+      bulk_g2s(dst + (size_t)nrows * S, filt + ((size_t)(b * a.atap + a_lo) * NMU) * S, fbytes, bar);
+  };
+  // phase p's data has arrived: buffer p & 1, used for the (p >> 1)-th time
+  auto wait_bulk = [&](int p) {
+    long long it = 0;
+    while (!mbar_try_wait(&s_mbar[p & 1], (unsigned)((p >> 1) & 1))) {
+      if (++it > kBulkWaitLimit) {
+        if (tid == 0) atomicExch(a.err, 1);
+        break;
+      }
+    }
+  };
+  if (BULK) {
+    if (tid == 0) {
+      mbar_init(&s_mbar[0], 1);
+      mbar_init(&s_mbar[1], 1);
+      mbar_init_fence();
+    }
+    __syncthreads();
+  }
 
   V acc[JR][NMU];
 #pragma unroll
@@ -280,11 +353,18 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_conv_sfft_tS(Conv2Args a)
 #pragma unroll
     for (int th = 0; th < NMU; ++th) acc[jj][th] = cmk<V>((R)0, (R)0);
 
-  issue(0, buf0);
-  cp_async_commit();
+  if (BULK) {
+    issue_bulk(0, buf0, &s_mbar[0]);
+  } else {
+    issue(0, buf0);
+    cp_async_commit();
+  }
   for (int p = 0; p < nphase; ++p) {
     V *cur = (p & 1) ? buf1 : buf0;
-    if (p + 1 < nphase) {
+    if (BULK) {
+      if (p + 1 < nphase) issue_bulk(p + 1, (p & 1) ? buf0 : buf1, &s_mbar[(p + 1) & 1]);
+      wait_bulk(p);
+    } else if (p + 1 < nphase) {
       issue(p + 1, (p & 1) ? buf0 : buf1);
       cp_async_commit();
       cp_async_wait<1>();

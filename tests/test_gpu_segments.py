@@ -203,3 +203,19 @@ def test_inverse_matches_direct_inverse_fft_and_round_trips(N, S, prec, tol):
         assert np.array_equal(yh, y.cpu().numpy())
     finally:
         d.free()
+
+
+def test_misaligned_device_input_is_rejected():
+    N, S, prec = 1 << 16, 8, sb.PRECISION_SPLIT_FP32
+    d = _desc(N, S, prec)
+    try:
+        big = torch.zeros(N + 1, dtype=torch.complex64, device="cuda")
+        x = big[1:]                                   # 8-byte aligned only
+        y = torch.empty(N, dtype=torch.complex64, device="cuda")
+        with pytest.raises(sb.SoiError) as e:
+            d.compute_into(x, y)
+        assert e.value.status == 1                    # SOI_ERR_INVALID
+        x2 = big[:N]
+        d.compute_into(x2, y)                         # the aligned view works
+    finally:
+        d.free()

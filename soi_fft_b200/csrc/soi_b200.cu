@@ -574,7 +574,10 @@ void plan_stage1_staged(Plan &p)
         p.s1fast = 1;
         p.s1_tS = ts ? 1 : 0;
         p.s1_nt = ts ? nt : 512;
-        p.s1_bulk = ts && nt == 512 && (p.knob_s1_bulk >= 0 ? p.knob_s1_bulk : env_int("SOI_STAGE1_BULK", 1)) ? 1 : 0;
+        // staging by bulk copies: correct, but measured slower at N = 2^29, S = 128
+        // (7.25 vs 6.36 ms: one warp's 42 serial row copies per phase arrive later
+        // than 512 threads' 16-byte cp.async); off unless asked for
+        p.s1_bulk = ts && nt == 512 && (p.knob_s1_bulk >= 0 ? p.knob_s1_bulk : env_int("SOI_STAGE1_BULK", 0)) ? 1 : 0;
         return;
       }
     }

@@ -219,3 +219,22 @@ def test_misaligned_device_input_is_rejected():
         d.compute_into(x2, y)                         # the aligned view works
     finally:
         d.free()
+
+
+@pytest.mark.parametrize("N,S,prec", [(1 << 20, 16, sb.PRECISION_SPLIT_FP32), (1 << 22, 128, sb.PRECISION_SPLIT_FP32),
+                                      (1 << 18, 8, sb.PRECISION_FP64)])
+def test_bulk_copy_staging_equals_cp_async_staging(N, S, prec, monkeypatch):
+    # the two ways of staging stage 1's input rows feed identical arithmetic
+    x = _input(N, prec)
+    outs = []
+    for bulk in ("0", "1"):
+        monkeypatch.setenv("SOI_STAGE1_BULK", bulk)
+        d = _desc(N, S, prec)
+        try:
+            y = torch.empty_like(x)
+            d.compute_into(x, y)
+            torch.cuda.synchronize()
+            outs.append(y)
+        finally:
+            d.free()
+    assert torch.equal(outs[0], outs[1])

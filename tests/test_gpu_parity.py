@@ -183,6 +183,26 @@ def test_large_sizes_against_cufft(N, S):
     assert float(torch.linalg.norm(lhs - rhs) / torch.linalg.norm(rhs)) <= FP64_TOL
 
 
+@pytest.mark.parametrize("N,S,prec", [(1 << 28, 64, "fp64"), (1 << 29, 128, "split")])
+def test_configured_sizes_against_cufft(N, S, prec):
+    # the configured workloads at full size: plain FP64 at N = 2^28, P = 64 and
+    # the split form at N = 2^29, P = 128, on Gaussian + 64 tones, against the
+    # FP64 direct FFT (cuFFT Z2Z, the checker)
+    xd = signals.gaussian_plus_tones_torch(N, 7)
+    X = torch.fft.fft(xd)
+    nX = torch.linalg.norm(X)
+    if prec == "fp64":
+        y = sb.soi_fft(xd, S)
+        assert float(torch.linalg.norm(y - X) / nX) <= FP64_TOL
+    else:
+        x32 = xd.to(torch.complex64)
+        del xd
+        y = sb.soi_fft(x32, S).to(torch.complex128)
+        assert float(torch.linalg.norm(y - X) / nX) <= SPLIT_TOL
+    del X, y
+    torch.cuda.empty_cache()
+
+
 def test_timings_reported():
     N, S = 1 << 20, 16
     d = sb.SoiDescriptor(N=N, precision=sb.PRECISION_SPLIT_FP32).init(S)

@@ -56,8 +56,8 @@ CPU_SAMPLE_LOG2N = 24
 # dram__bytes_write.sum; the traffic grows with the units processed, so the
 # ratio carries to N = 2^29).  None where no capture backs a figure.
 KERNELS = {
-    "stage1": ("k_conv_sfft_tS (stage 1: convolution + S-point FFTs + transposed store)", 1160.5 / 1208.0),
-    "stage2": ("k_stage2_ct (stage 2: M'-point four-step FFT + demodulation + discard)", 1165.9 / 1208.0),
+    "stage1": ("k_conv_sfft_tS (stage 1: convolution + S-point FFTs + transposed store)", 1163.2 / 1208.0),
+    "stage2": ("k_stage2_ct (stage 2: M'-point four-step FFT + demodulation + discard)", 1163.3 / 1208.0),
 }
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the same kernel at N=2^26, S=128 "
                   "(profiles/k_conv_sfft_tS_N2e26_S128_split.md, profiles/k_stage2_ct_N2e26_S128_split.md), "
@@ -81,7 +81,7 @@ def parse():
     ap.add_argument("--workload", default="headline", choices=["headline", "batched"],
                     help="batched: the band-limited batch of mixed lengths (its own JSON line)")
     ap.add_argument("--batch-count", type=int, default=4096)
-    ap.add_argument("--batch-chains", type=int, default=4)
+    ap.add_argument("--batch-chains", type=int, default=8)
     return ap.parse_args()
 
 

@@ -464,7 +464,7 @@ int launch_conv2_t(Plan &p, const Exec &ex)
 // staged stage-1 instances: (precision, n_mu) -> JR
 int staged_jr(int prec, int nmu)
 {
-  if (prec == SOI_PRECISION_SPLIT_FP32) return nmu == 5 ? 6 : nmu == 3 ? 6 : (nmu == 8 || nmu == 9) ? 4 : 0;
+  if (prec == SOI_PRECISION_SPLIT_FP32) return nmu == 5 ? 8 : nmu == 3 ? 6 : (nmu == 8 || nmu == 9) ? 4 : 0;
   return nmu == 5 ? 4 : nmu == 3 ? 4 : (nmu == 8 || nmu == 9) ? 2 : 0;
 }
 
@@ -520,11 +520,11 @@ int tS_r1(size_t S) { return S == 8 ? 4 : S == 16 ? 4 : S == 32 ? 8 : S == 64 ? 
 int launch_conv2(Plan &p, const Exec &ex)
 {
   if (p.s1_tS)
-    return p.prec == SOI_PRECISION_SPLIT_FP32 ? launch_tS_switch<float, 6>(p, ex)
+    return p.prec == SOI_PRECISION_SPLIT_FP32 ? launch_tS_switch<float, 8>(p, ex)
                                               : launch_tS_switch<double, 4>(p, ex);
   if (p.prec == SOI_PRECISION_SPLIT_FP32) {
     switch (p.nmu) {
-      case 5: return launch_conv2_t<float, 5, 6>(p, ex);
+      case 5: return launch_conv2_t<float, 5, 8>(p, ex);
       case 3: return launch_conv2_t<float, 3, 6>(p, ex);
       case 8: return launch_conv2_t<float, 8, 4>(p, ex);
       case 9: return launch_conv2_t<float, 9, 4>(p, ex);

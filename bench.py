@@ -390,7 +390,7 @@ def run_ours(args):
     h_in = torch.empty(N, dtype=torch.complex64, pin_memory=True)
     h_in.copy_(x32)
     h_out = torch.empty(N, dtype=torch.complex64, pin_memory=True)
-    e2e_steps = max(3, min(args.steps, 6))
+    e2e_steps = max(3, min(args.steps, 10))
     hi, ho = h_in.numpy(), h_out.numpy()
     d32.compute_stream([hi], [ho])
     e2e_matches = bool(torch.equal(h_out, y32.cpu()))

@@ -81,7 +81,7 @@ def parse():
     ap.add_argument("--workload", default="headline", choices=["headline", "batched"],
                     help="batched: the band-limited batch of mixed lengths (its own JSON line)")
     ap.add_argument("--batch-count", type=int, default=4096)
-    ap.add_argument("--batch-chains", type=int, default=8)
+    ap.add_argument("--batch-chains", type=int, default=16)
     return ap.parse_args()
 
 

@@ -82,6 +82,8 @@ def parse():
                     help="batched: the band-limited batch of mixed lengths (its own JSON line)")
     ap.add_argument("--batch-count", type=int, default=4096)
     ap.add_argument("--batch-chains", type=int, default=16)
+    ap.add_argument("--vlc", action="store_true",
+                    help="with the VLC round trip between the stages (use_vlc = 1, pfft.c:316-353,618-632)")
     return ap.parse_args()
 
 
@@ -328,7 +330,7 @@ def run_ours(args):
     x32 = x128.to(torch.complex64)
 
     def new_desc(prec):
-        d = sb.SoiDescriptor(N=N, precision=prec, device=local, stream=stream.cuda_stream)
+        d = sb.SoiDescriptor(N=N, precision=prec, device=local, stream=stream.cuda_stream, use_vlc=int(args.vlc))
         d.init(S)
         return d
 
@@ -375,6 +377,7 @@ def run_ours(args):
     _, st = timed(d32, x32, y32, max(2, args.steps // 2), 0, per_stage=True)
     stage1 = statistics.mean(s["stage1_ms"] for s in st)
     stage2 = statistics.mean(s["stage2_ms"] for s in st)
+    vlc_ms = statistics.mean(s["vlc_ms"] for s in st)
 
     # ---- accuracy vs the FP64 direct FFT (cuFFT Z2Z, checker only)
     X = torch.fft.fft(x128)
@@ -439,7 +442,7 @@ def run_ours(args):
                 "traffic": traffic_ratio * alg_bytes if traffic_ratio else None,
                 "traffic_source": TRAFFIC_SOURCE if traffic_ratio else None,
                 "algorithmic_bytes_per_launch": alg_bytes,
-                "stage1_ms": stage1, "stage2_ms": stage2,
+                "stage1_ms": stage1, "stage2_ms": stage2, "vlc_ms": vlc_ms if args.vlc else None,
                 "pipeline_achieved_gbs": 2 * alg_bytes / (ms_step / 1e3) / 1e9}
 
     cpu = None
@@ -456,8 +459,9 @@ def run_ours(args):
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic: seeded complex Gaussian + 64 tones, amplitudes log-uniform [1e-6, 1]",
-                "config": {"workload": "SOI FFT split-precision, N=2^%d complex64, S=%d, mu=5/4, B=72"
-                                       % (args.log2n, S),
+                "config": {"workload": "SOI FFT split-precision, N=2^%d complex64, S=%d, mu=5/4, B=72%s"
+                                       % (args.log2n, S, ", VLC round trip" if args.vlc else ""),
+                           "use_vlc": bool(args.vlc),
                            "N": N, "S": S, "mu": "5/4", "B": 72, "precision": "split_fp32",
                            "l2": "inputs (%d MiB) larger than L2 (126 MB), no flush" % (N * 8 >> 20),
                            "parallelism": "replicas x%d" % world},

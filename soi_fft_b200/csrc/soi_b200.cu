@@ -910,8 +910,7 @@ int run_vlc(Plan &p, const Exec &ex)
     vlc_promote<<<1024, 256, 0, st>>>((const float *)T, x, (long long)len * ns);
     CK(cudaGetLastError());
   }
-  vlc_max_exponent_kernel<<<ns, 256, 0, st>>>(x, len, p.d_vlc_emax);
-  CK(cudaGetLastError());
+  CK(vlc_max_exponent(x, len, ns, p.d_vlc_emax, st));
   vlc_global_max<<<1, 256, 0, st>>>(p.d_vlc_emax, ns, p.d_vlc_emax + ns);
   CK(cudaGetLastError());
   dim3 gv(64, (unsigned)ns);
@@ -1541,8 +1540,7 @@ int soi_vlc_words(int len, int e_max, int e_max_i)
 int soi_vlc_max_exponent_device(const double *x, int len, int nchunks, int *e_max_out, void *stream)
 {
   if (!x || !e_max_out || len <= 0 || nchunks <= 0) return SOI_ERR_INVALID;
-  vlc_max_exponent_kernel<<<nchunks, 256, 0, (cudaStream_t)stream>>>(x, len, e_max_out);
-  CK(cudaGetLastError());
+  CK(vlc_max_exponent(x, len, nchunks, e_max_out, (cudaStream_t)stream));
   return SOI_OK;
 }
 
@@ -1752,11 +1750,11 @@ extern "C" int soi_vlc_roundtrip_noalloc_device(const double *x_dev, double *out
   int *nwords = scr + kNoallocMaxChunks + 1;
   int *words = scr + kNoallocHeaderInts;    // [nchunks][per_chunk]
   cudaStream_t st = (cudaStream_t)stream;
-  // every scratch entry read below is written earlier in this call (exponents,
-  // maximum, counts, and each compressed word including its zero padding), so
-  // nothing has to be cleared first
-  vlc_max_exponent_kernel<<<nchunks, 256, 0, st>>>(x_dev, len, e_max_i);
-  CK(cudaGetLastError());
+  // every scratch entry read below is written earlier in this call (the
+  // exponents, preset and then maximised by vlc_max_exponent, the maximum, the
+  // counts, and each compressed word including its zero padding), so nothing
+  // else has to be cleared first
+  CK(vlc_max_exponent(x_dev, len, nchunks, e_max_i, st));
   vlc_global_max<<<1, 256, 0, st>>>(e_max_i, nchunks, g_max);
   CK(cudaGetLastError());
   dim3 g(64, (unsigned)nchunks);

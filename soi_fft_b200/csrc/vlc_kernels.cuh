@@ -8,10 +8,12 @@
 // lane's 32-bit words; lane L's word w is stored at out[16*w + L]; a partial
 // last word group is flushed with zero padding.  Because every lane receives
 // the same number of bits, bit b of lane L's stream is simply bit (b mod 32,
-// from the top) of word floor(b/32) -- so each output word can be assembled
-// independently from the (at most ceil(32/nb)+1) fields it overlaps, and each
-// element decoded independently from the (at most 3) words its field spans.
-// That is what these kernels do: one thread per word, one thread per element.
+// from the top) of word floor(b/32).  32 consecutive fields of a lane fill
+// exactly nb whole words, so a lane's stream splits into independent units of
+// 32 fields / nb words: the kernels give each thread one unit (lane L, block
+// k), which it packs or unpacks sequentially with no division and no word
+// shared with another thread; only a chunk's last unit may be partial (its
+// last word zero-padded).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -73,12 +75,16 @@ __global__ void vlc_demote(const double *in, float *out, long long n)
     out[i] = (float)in[i];
 }
 
-// compress.c:11-131: per chunk (blockIdx.x), max biased exponent - 1023.
+// compress.c:11-131: per chunk (blockIdx.y), max biased exponent - 1023.
+// Several blocks per chunk (blockIdx.x, grid-stride); each folds its maximum
+// into e_max[chunk] with atomicMax, so e_max must start below any result
+// (vlc_max_exponent below presets it).
 __global__ void vlc_max_exponent_kernel(const double *x, int len, int *e_max)
 {
-  const double *c = x + (size_t)blockIdx.x * len;
+  const double *c = x + (size_t)blockIdx.y * len;
   int m = 0;
-  for (int i = threadIdx.x; i < len; i += blockDim.x) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len;
+       i += (long long)gridDim.x * blockDim.x) {
     const unsigned long long u = (unsigned long long)__double_as_longlong(c[i]);
     m = max(m, (int)((u >> 52) & 0x7FF));
   }
@@ -89,8 +95,20 @@ __global__ void vlc_max_exponent_kernel(const double *x, int len, int *e_max)
   if (threadIdx.x < 32) {
     int v = threadIdx.x < (blockDim.x + 31) / 32 ? wm[threadIdx.x] : 0;
     for (int o = 16; o; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
-    if (threadIdx.x == 0) e_max[blockIdx.x] = v - 1023;
+    if (threadIdx.x == 0) atomicMax(e_max + blockIdx.y, v - 1023);
   }
+}
+
+// Per-chunk maximum exponents of nchunks chunks of len doubles into e_max.
+inline cudaError_t vlc_max_exponent(const double *x, int len, int nchunks, int *e_max, cudaStream_t st)
+{
+  // 0x80 bytes: every preset word is far below -1023, the smallest result
+  cudaError_t e = cudaMemsetAsync(e_max, 0x80, (size_t)nchunks * sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  const long long per = ((long long)len + 2047) / 2048;
+  dim3 g((unsigned)(per < 64 ? per : 64), (unsigned)nchunks);
+  vlc_max_exponent_kernel<<<g, 256, 0, st>>>(x, len, e_max);
+  return cudaGetLastError();
 }
 
 // max over chunks (pfft.c:340-343, after the MPI_Allreduce MAX of :331-333)
@@ -119,8 +137,9 @@ __host__ __device__ __forceinline__ long long vlc_words_per_lane(int len, int nb
   return (groups * nb + 31) / 32;
 }
 
-// compress.c:205-372, one chunk per blockIdx.y (grid-stride over words in x).
-// e_max = *e_max_dev when given, else e_max_host; e_max_i[c] per chunk.
+// compress.c:205-372, one chunk per blockIdx.y; one thread per unit (lane L,
+// block k of 32 fields), grid-stride over the chunk's units.  e_max =
+// *e_max_dev when given, else e_max_host; e_max_i[c] per chunk.
 __global__ void vlc_compress_kernel(const double *x, int len, int e_max_host, const int *e_max_dev,
                                     const int *e_max_i, int *words, long stride, int *nwords)
 {
@@ -128,41 +147,48 @@ __global__ void vlc_compress_kernel(const double *x, int len, int e_max_host, co
   const int e_max = e_max_dev ? *e_max_dev : e_max_host;
   const VlcBits b = vlc_bits(e_max, e_max_i[c]);
   const double *xc = x + (size_t)c * len;
-  int *wc = words + (size_t)c * stride;
+  uint32_t *wc = reinterpret_cast<uint32_t *>(words + (size_t)c * stride);
   if (b.i2Len <= 0) {                        // compress.c:210-212
     if (blockIdx.x == 0 && threadIdx.x == 0) nwords[c] = 0;
     return;
   }
-  const long long nwl = vlc_words_per_lane(len, b.nb);
-  const long long total = nwl * kVlcLanes;
+  const int nb = b.nb;
   const long long groups = len / kVlcLanes;
-  if (blockIdx.x == 0 && threadIdx.x == 0) nwords[c] = (int)total;
-  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
-       idx += (long long)gridDim.x * blockDim.x) {
-    const long long w = idx / kVlcLanes;
-    const int L = (int)(idx % kVlcLanes);
-    const long long sb = 32 * w;                // first stream bit of the word
-    long long g = sb / b.nb;
-    int skip = (int)(sb - g * b.nb);           // bits of field g already used
-    uint32_t word = 0;
-    int have = 0;                               // bits placed so far (from the top)
-    while (have < 32 && g < groups) {
-      const uint64_t f = vlc_field(xc[g * kVlcLanes + L], b);
-      const int avail = b.nb - skip;            // remaining bits of this field
-      const int take = min(avail, 32 - have);
-      // bits [avail-1 .. avail-take] of the field's remaining low bits
-      const uint64_t part = (f >> (avail - take)) & ((1ull << take) - 1);
-      word |= (uint32_t)(part << (32 - have - take));
-      have += take;
-      ++g;
-      skip = 0;
+  const long long nblk = (groups + 31) / 32;
+  if (blockIdx.x == 0 && threadIdx.x == 0) nwords[c] = (int)(vlc_words_per_lane(len, nb) * kVlcLanes);
+  for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < nblk * kVlcLanes;
+       u += (long long)gridDim.x * blockDim.x) {
+    const int L = (int)(u % kVlcLanes);
+    const long long k = u / kVlcLanes;
+    const long long g0 = 32 * k;
+    const int nf = (int)(groups - g0 < 32 ? groups - g0 : 32);
+    const double *src = xc + g0 * kVlcLanes + L;
+    uint32_t *dst = wc + (size_t)k * nb * kVlcLanes + L;          // word k*nb of lane L
+    uint32_t cur = 0;
+    int have = 0;                                                // bits placed in cur, from the top
+    for (int j = 0; j < nf; ++j) {
+      const uint64_t f = vlc_field(src[(size_t)j * kVlcLanes], b);
+      int rem = nb;
+      while (rem > 0) {
+        const int take = min(32 - have, rem);
+        const uint32_t part = (uint32_t)((f >> (rem - take)) & ((1ull << take) - 1));
+        cur |= part << (32 - have - take);
+        have += take;
+        rem -= take;
+        if (have == 32) {
+          *dst = cur;
+          dst += kVlcLanes;
+          cur = 0;
+          have = 0;
+        }
+      }
     }
-    wc[idx] = (int)word;
+    if (have > 0) *dst = cur;                                    // last unit: zero-padded word
   }
 }
 
-// compress.c:428-544 (vector body, :395-426 and :450-489), one element per
-// thread, one chunk per blockIdx.y.
+// compress.c:428-544 (vector body, :395-426 and :450-489), one chunk per
+// blockIdx.y; one thread per unit (lane L, block k of 32 fields).
 __global__ void vlc_decompress_kernel(const int *words, long stride, int len, const int *unused,
                                       const int *e_max_dev, const int *e_max_i, double *out)
 {
@@ -172,35 +198,47 @@ __global__ void vlc_decompress_kernel(const int *words, long stride, int len, co
   const VlcBits b = vlc_bits(e_max, e_max_i[c]);
   double *oc = out + (size_t)c * len;
   const uint32_t *wc = reinterpret_cast<const uint32_t *>(words + (size_t)c * stride);
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < len;
-       e += (long long)gridDim.x * blockDim.x) {
-    if (b.i2Len <= 0) { oc[e] = 0.0; continue; }
-    const long long g = e / kVlcLanes;
-    const int L = (int)(e % kVlcLanes);
-    const long long sb = g * b.nb;
-    long long w = sb / 32;
-    int off = (int)(sb - 32 * w);               // bit offset from the top of word w
-    // gather nb bits MSB-first into f
-    uint64_t f = 0;
-    int need = b.nb;
-    while (need > 0) {
-      const uint32_t word = __ldg(wc + w * kVlcLanes + L);
-      const int avail = 32 - off;
-      const int take = min(avail, need);
-      const uint32_t part = (uint32_t)(((uint64_t)word >> (avail - take)) & ((1ull << take) - 1));
-      f = (f << take) | part;
-      need -= take;
-      ++w;
-      off = 0;
+  const int nb = b.nb;
+  const long long groups = len / kVlcLanes;
+  const long long nblk = (groups + 31) / 32;
+  for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < nblk * kVlcLanes;
+       u += (long long)gridDim.x * blockDim.x) {
+    const int L = (int)(u % kVlcLanes);
+    const long long k = u / kVlcLanes;
+    const long long g0 = 32 * k;
+    const int nf = (int)(groups - g0 < 32 ? groups - g0 : 32);
+    double *dst = oc + g0 * kVlcLanes + L;
+    if (b.i2Len <= 0) {
+      for (int j = 0; j < nf; ++j) dst[(size_t)j * kVlcLanes] = 0.0;
+      continue;
     }
-    int32_t i1 = 0;
-    if (b.i1Len > 0) {
-      const uint32_t top = (uint32_t)(f >> b.i2Len);
-      i1 = (int32_t)(top << (32 - b.i1Len)) >> (32 - b.i1Len);
+    const uint32_t *src = wc + (size_t)k * nb * kVlcLanes + L;
+    uint32_t cur = 0;
+    int left = 0;                                                // unread bits of cur, at its bottom
+    for (int j = 0; j < nf; ++j) {
+      // gather nb bits MSB-first into f
+      uint64_t f = 0;
+      int need = nb;
+      while (need > 0) {
+        if (left == 0) {
+          cur = __ldg(src);
+          src += kVlcLanes;
+          left = 32;
+        }
+        const int take = min(left, need);
+        f = (f << take) | (((uint64_t)cur >> (left - take)) & ((1ull << take) - 1));
+        left -= take;
+        need -= take;
+      }
+      int32_t i1 = 0;
+      if (b.i1Len > 0) {
+        const uint32_t top = (uint32_t)(f >> b.i2Len);
+        i1 = (int32_t)(top << (32 - b.i1Len)) >> (32 - b.i1Len);
+      }
+      const uint32_t low = (uint32_t)(f & (b.i2Len >= 32 ? 0xFFFFFFFFull : ((1ull << b.i2Len) - 1)));
+      const int32_t i2 = b.i2Len >= 32 ? (int32_t)low : ((int32_t)(low << (32 - b.i2Len)) >> (32 - b.i2Len));
+      dst[(size_t)j * kVlcLanes] = fma((double)i1, b.d1, __dmul_rn((double)i2, b.d2));
     }
-    const uint32_t low = (uint32_t)(f & (b.i2Len >= 32 ? 0xFFFFFFFFull : ((1ull << b.i2Len) - 1)));
-    const int32_t i2 = b.i2Len >= 32 ? (int32_t)low : ((int32_t)(low << (32 - b.i2Len)) >> (32 - b.i2Len));
-    oc[e] = fma((double)i1, b.d1, __dmul_rn((double)i2, b.d2));
   }
 }
 

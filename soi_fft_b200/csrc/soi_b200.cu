@@ -49,7 +49,6 @@ struct Plan {
   cudaStream_t st_in = nullptr, st_out = nullptr;   // copy streams (streamed host transforms)
   cudaEvent_t sev[6] = {};     // in-copied[2], computed[2], out-copied[2]
   // VLC
-  double *d_vlc_x = nullptr;   // promoted/decompressed doubles (FP32 path)
   int *d_vlc_words = nullptr, *d_vlc_n = nullptr, *d_vlc_emax = nullptr;
   long vlc_stride = 0;
   // persistent stage 2: compiled radix split and its state
@@ -712,7 +711,7 @@ void free_plan(Plan *p)
   cudaSetDevice(p->device);
   void *bufs[] = { p->d_filt, p->d_phase, p->d_twS, p->d_tw1, p->d_tw2, p->d_winv, p->d_wsmall,
                    p->d_permS, p->d_perm1, p->d_perm2, p->d_xlo, p->d_xhi, p->d_T, p->d_io, p->d_io2,
-                   p->d_vlc_x, p->d_vlc_words, p->d_vlc_n, p->d_vlc_emax, p->d_sync, p->d_filt2, p->d_amp, p->d_dlo, p->d_dhi, p->d_ph2 };
+                   p->d_vlc_words, p->d_vlc_n, p->d_vlc_emax, p->d_sync, p->d_filt2, p->d_amp, p->d_dlo, p->d_dhi, p->d_ph2 };
   for (void *b : bufs) if (b) cudaFree(b);
   for (auto &e : p->ev) if (e) cudaEventDestroy(e);
   for (auto &e : p->sev) if (e) cudaEventDestroy(e);
@@ -891,7 +890,6 @@ int vlc_alloc(Plan &p)
   CK(cudaMalloc(&p.d_vlc_words, (size_t)p.vlc_stride * S * sizeof(int)));
   CK(cudaMalloc(&p.d_vlc_n, S * sizeof(int)));
   CK(cudaMalloc(&p.d_vlc_emax, (S + 1) * sizeof(int)));
-  if (p.prec != SOI_PRECISION_FP64) CK(cudaMalloc(&p.d_vlc_x, len * S * sizeof(double)));
   return SOI_OK;
 }
 
@@ -905,25 +903,31 @@ int run_vlc(Plan &p, const Exec &ex)
   const int ns = ex.hi - ex.lo;
   int rc;
   if ((rc = vlc_alloc(p))) return rc;
-  double *x = p.prec == SOI_PRECISION_FP64 ? (double *)T : p.d_vlc_x;
-  if (p.prec != SOI_PRECISION_FP64) {
-    vlc_promote<<<1024, 256, 0, st>>>((const float *)T, x, (long long)len * ns);
-    CK(cudaGetLastError());
-  }
-  CK(vlc_max_exponent(x, len, ns, p.d_vlc_emax, st));
+  // the split form's floats are read and written in place (widened to double
+  // in the kernels, exactly), so no promoted copy is made
+  CK(p.prec == SOI_PRECISION_FP64 ? vlc_max_exponent((const double *)T, len, ns, p.d_vlc_emax, st)
+                                  : vlc_max_exponent((const float *)T, len, ns, p.d_vlc_emax, st));
   vlc_global_max<<<1, 256, 0, st>>>(p.d_vlc_emax, ns, p.d_vlc_emax + ns);
   CK(cudaGetLastError());
   dim3 gv(64, (unsigned)ns);
-  vlc_compress_kernel<<<gv, 256, vlc_compress_smem(), st>>>(x, len, 0, p.d_vlc_emax + ns, p.d_vlc_emax,
-                                                           p.d_vlc_words, p.vlc_stride, p.d_vlc_n);
-  CK(cudaGetLastError());
-  vlc_decompress_kernel<<<gv, 256, vlc_decompress_smem(), st>>>(p.d_vlc_words, p.vlc_stride, len, nullptr,
-                                                               p.d_vlc_emax + ns, p.d_vlc_emax, x);
-  CK(cudaGetLastError());
-  if (p.prec != SOI_PRECISION_FP64) {
-    vlc_demote<<<1024, 256, 0, st>>>(x, (float *)T, (long long)len * ns);
+  if (p.prec == SOI_PRECISION_FP64) {
+    vlc_compress_kernel<double><<<gv, 256, vlc_compress_smem(), st>>>((const double *)T, len, 0, p.d_vlc_emax + ns,
+                                                                      p.d_vlc_emax, p.d_vlc_words, p.vlc_stride,
+                                                                      p.d_vlc_n);
     CK(cudaGetLastError());
+    vlc_decompress_kernel<double><<<gv, 256, vlc_decompress_smem(), st>>>(p.d_vlc_words, p.vlc_stride, len, nullptr,
+                                                                          p.d_vlc_emax + ns, p.d_vlc_emax,
+                                                                          (double *)T);
+  } else {
+    vlc_compress_kernel<float><<<gv, 256, vlc_compress_smem(), st>>>((const float *)T, len, 0, p.d_vlc_emax + ns,
+                                                                     p.d_vlc_emax, p.d_vlc_words, p.vlc_stride,
+                                                                     p.d_vlc_n);
+    CK(cudaGetLastError());
+    vlc_decompress_kernel<float><<<gv, 256, vlc_decompress_smem(), st>>>(p.d_vlc_words, p.vlc_stride, len, nullptr,
+                                                                         p.d_vlc_emax + ns, p.d_vlc_emax,
+                                                                         (float *)T);
   }
+  CK(cudaGetLastError());
   return SOI_OK;
 }
 
@@ -1460,7 +1464,7 @@ int soi_kernels_per_compute(soi_desc_t *d)
   Plan *p = plan_of(d);
   if (!p) return -SOI_ERR_NOT_INITIALISED;
   int n = 1 + (p->fast2 ? 1 : 2);
-  if (d->use_vlc) n += p->prec == SOI_PRECISION_FP64 ? 4 : 6;   // run_vlc
+  if (d->use_vlc) n += 4;                                       // run_vlc
   return n;
 }
 
@@ -1643,7 +1647,7 @@ int soi_batch_info(soi_batch_t *batch, long long *info)
   long long launches = 0;
   for (auto &it : b->items) {
     const Plan &p = *b->plans[it.plan];
-    launches += 1 + (p.fast2 ? 1 : 2) + (b->tmpl.use_vlc ? (p.prec == SOI_PRECISION_FP64 ? 4 : 6) : 0);
+    launches += 1 + (p.fast2 ? 1 : 2) + (b->tmpl.use_vlc ? 4 : 0);
   }
   info[4] = launches;
   size_t scratch = 0;

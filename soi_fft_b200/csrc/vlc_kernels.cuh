@@ -63,29 +63,20 @@ __device__ __forceinline__ uint64_t vlc_field(double x, const VlcBits &b)
   return f;
 }
 
-__global__ void vlc_promote(const float *in, double *out, long long n)
-{
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    out[i] = (double)in[i];
-}
-
-__global__ void vlc_demote(const double *in, float *out, long long n)
-{
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    out[i] = (float)in[i];
-}
-
 // compress.c:11-131: per chunk (blockIdx.y), max biased exponent - 1023.
 // Several blocks per chunk (blockIdx.x, grid-stride); each folds its maximum
 // into e_max[chunk] with atomicMax, so e_max must start below any result
 // (vlc_max_exponent below presets it).
-__global__ void vlc_max_exponent_kernel(const double *x, int len, int *e_max)
+// X = double, or float for the split form's data (each value widened to
+// double exactly, as the round trip defines it on doubles).
+template <typename X>
+__global__ void vlc_max_exponent_kernel(const X *x, int len, int *e_max)
 {
-  const double *c = x + (size_t)blockIdx.y * len;
+  const X *c = x + (size_t)blockIdx.y * len;
   int m = 0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len;
        i += (long long)gridDim.x * blockDim.x) {
-    const unsigned long long u = (unsigned long long)__double_as_longlong(c[i]);
+    const unsigned long long u = (unsigned long long)__double_as_longlong((double)c[i]);
     m = max(m, (int)((u >> 52) & 0x7FF));
   }
   for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
@@ -100,14 +91,15 @@ __global__ void vlc_max_exponent_kernel(const double *x, int len, int *e_max)
 }
 
 // Per-chunk maximum exponents of nchunks chunks of len doubles into e_max.
-inline cudaError_t vlc_max_exponent(const double *x, int len, int nchunks, int *e_max, cudaStream_t st)
+template <typename X>
+inline cudaError_t vlc_max_exponent(const X *x, int len, int nchunks, int *e_max, cudaStream_t st)
 {
   // 0x80 bytes: every preset word is far below -1023, the smallest result
   cudaError_t e = cudaMemsetAsync(e_max, 0x80, (size_t)nchunks * sizeof(int), st);
   if (e != cudaSuccess) return e;
   const long long per = ((long long)len + 2047) / 2048;
   dim3 g((unsigned)(per < 64 ? per : 64), (unsigned)nchunks);
-  vlc_max_exponent_kernel<<<g, 256, 0, st>>>(x, len, e_max);
+  vlc_max_exponent_kernel<X><<<g, 256, 0, st>>>(x, len, e_max);
   return cudaGetLastError();
 }
 
@@ -140,13 +132,14 @@ __host__ __device__ __forceinline__ long long vlc_words_per_lane(int len, int nb
 // compress.c:205-372, one chunk per blockIdx.y; one thread per unit (lane L,
 // block k of 32 fields), grid-stride over the chunk's units.  e_max =
 // *e_max_dev when given, else e_max_host; e_max_i[c] per chunk.
-__global__ void vlc_compress_kernel(const double *x, int len, int e_max_host, const int *e_max_dev,
+template <typename X>
+__global__ void vlc_compress_kernel(const X *x, int len, int e_max_host, const int *e_max_dev,
                                     const int *e_max_i, int *words, long stride, int *nwords)
 {
   const int c = blockIdx.y;
   const int e_max = e_max_dev ? *e_max_dev : e_max_host;
   const VlcBits b = vlc_bits(e_max, e_max_i[c]);
-  const double *xc = x + (size_t)c * len;
+  const X *xc = x + (size_t)c * len;
   uint32_t *wc = reinterpret_cast<uint32_t *>(words + (size_t)c * stride);
   if (b.i2Len <= 0) {                        // compress.c:210-212
     if (blockIdx.x == 0 && threadIdx.x == 0) nwords[c] = 0;
@@ -162,12 +155,12 @@ __global__ void vlc_compress_kernel(const double *x, int len, int e_max_host, co
     const long long k = u / kVlcLanes;
     const long long g0 = 32 * k;
     const int nf = (int)(groups - g0 < 32 ? groups - g0 : 32);
-    const double *src = xc + g0 * kVlcLanes + L;
+    const X *src = xc + g0 * kVlcLanes + L;
     uint32_t *dst = wc + (size_t)k * nb * kVlcLanes + L;          // word k*nb of lane L
     uint32_t cur = 0;
     int have = 0;                                                // bits placed in cur, from the top
     for (int j = 0; j < nf; ++j) {
-      const uint64_t f = vlc_field(src[(size_t)j * kVlcLanes], b);
+      const uint64_t f = vlc_field((double)src[(size_t)j * kVlcLanes], b);
       int rem = nb;
       while (rem > 0) {
         const int take = min(32 - have, rem);
@@ -189,14 +182,16 @@ __global__ void vlc_compress_kernel(const double *x, int len, int e_max_host, co
 
 // compress.c:428-544 (vector body, :395-426 and :450-489), one chunk per
 // blockIdx.y; one thread per unit (lane L, block k of 32 fields).
+// Y = double, or float for the split form (the decoded double rounded to float)
+template <typename Y>
 __global__ void vlc_decompress_kernel(const int *words, long stride, int len, const int *unused,
-                                      const int *e_max_dev, const int *e_max_i, double *out)
+                                      const int *e_max_dev, const int *e_max_i, Y *out)
 {
   (void)unused;
   const int c = blockIdx.y;
   const int e_max = *e_max_dev;
   const VlcBits b = vlc_bits(e_max, e_max_i[c]);
-  double *oc = out + (size_t)c * len;
+  Y *oc = out + (size_t)c * len;
   const uint32_t *wc = reinterpret_cast<const uint32_t *>(words + (size_t)c * stride);
   const int nb = b.nb;
   const long long groups = len / kVlcLanes;
@@ -207,9 +202,9 @@ __global__ void vlc_decompress_kernel(const int *words, long stride, int len, co
     const long long k = u / kVlcLanes;
     const long long g0 = 32 * k;
     const int nf = (int)(groups - g0 < 32 ? groups - g0 : 32);
-    double *dst = oc + g0 * kVlcLanes + L;
+    Y *dst = oc + g0 * kVlcLanes + L;
     if (b.i2Len <= 0) {
-      for (int j = 0; j < nf; ++j) dst[(size_t)j * kVlcLanes] = 0.0;
+      for (int j = 0; j < nf; ++j) dst[(size_t)j * kVlcLanes] = (Y)0;
       continue;
     }
     const uint32_t *src = wc + (size_t)k * nb * kVlcLanes + L;
@@ -237,7 +232,7 @@ __global__ void vlc_decompress_kernel(const int *words, long stride, int len, co
       }
       const uint32_t low = (uint32_t)(f & (b.i2Len >= 32 ? 0xFFFFFFFFull : ((1ull << b.i2Len) - 1)));
       const int32_t i2 = b.i2Len >= 32 ? (int32_t)low : ((int32_t)(low << (32 - b.i2Len)) >> (32 - b.i2Len));
-      dst[(size_t)j * kVlcLanes] = fma((double)i1, b.d1, __dmul_rn((double)i2, b.d2));
+      dst[(size_t)j * kVlcLanes] = (Y)fma((double)i1, b.d1, __dmul_rn((double)i2, b.d2));
     }
   }
 }

@@ -324,6 +324,61 @@ def evaluate(net, log2n=26, S=32, targets=(1e-12, 1e-11, 1e-10, 1e-9, 1e-8, 1e-7
             yield rec
 
 
+def evaluate_split(net, log2n=26, S=128, target=1e-6, seed=99, reps=5):
+    """The split form at one accuracy target: the default window (B = 72), the
+    analytic window and the learned window, each with its measured rel-L2 of the
+    split transform against the FP64 direct FFT and its median time.  The window
+    is chosen on the FP64 transform at target/4 (the split form adds ~3.5e-7 of
+    its own rounding), and accepted only if the split transform meets the
+    target.  Yields one dict per oversampling pair."""
+    import torch
+    from . import PRECISION_SPLIT_FP32
+
+    def run(x32, X, n_mu, d_mu, B, tau, sigma):
+        d = SoiDescriptor(N=x32.numel(), n_mu=n_mu, d_mu=d_mu, B=int(B), tau=float(tau), sigma=float(sigma),
+                          precision=PRECISION_SPLIT_FP32, device=x32.device.index or 0)
+        try:
+            d.init(S)
+            y = torch.empty_like(x32)
+            d.compute_into(x32, y)
+            ts = []
+            for _ in range(reps):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                a.record()
+                d.compute_into(x32, y)
+                b.record()
+                torch.cuda.synchronize()
+                ts.append(a.elapsed_time(b))
+        finally:
+            d.free()
+        e = float(torch.linalg.norm(y.to(torch.complex128) - X) / torch.linalg.norm(X))
+        return e, float(np.median(ts))
+
+    for (n_mu, d_mu) in MU_PAIRS:
+        N = length_for(n_mu, d_mu, log2n)
+        g = torch.Generator(device="cuda").manual_seed(seed + n_mu)
+        x = torch.complex(torch.randn(N, generator=g, device="cuda", dtype=torch.float64),
+                          torch.randn(N, generator=g, device="cuda", dtype=torch.float64))
+        X = torch.fft.fft(x)
+        x32 = x.to(torch.complex64)
+        measure = lambda B, tau, sigma: measure_error(x, S, n_mu, d_mu, int(B), tau, sigma, X)
+        rec = {"mu": "%d/%d" % (n_mu, d_mu), "N": N, "S": S, "target": target}
+        wins = {"default": (72, 928 / 1024., 373.7314)}
+        base = analytic_window(n_mu, d_mu, target / 4, measure)
+        if base[3] <= target / 4:
+            wins["analytic"] = base[:3]
+        learned = learned_window(net, n_mu, d_mu, target / 4, measure)
+        if learned is not None:
+            wins["learned"] = learned[:3]
+        for name, (B, tau, sigma) in wins.items():
+            e, ms = run(x32, X, n_mu, d_mu, B, tau, sigma)
+            rec[name] = {"B": int(B), "tau": tau, "sigma": sigma, "split_rel_l2": e, "ms": ms, "meets": e <= target}
+        del x, X, x32
+        torch.cuda.empty_cache()
+        yield rec
+
+
 def main():
     import argparse
     import json
@@ -337,10 +392,17 @@ def main():
     ap.add_argument("--evaluate", action="store_true",
                     help="evaluate the weights in --out against the analytic window instead of training")
     ap.add_argument("--eval-log2n", type=int, default=26)
+    ap.add_argument("--evaluate-split", type=float, default=None, metavar="TARGET",
+                    help="time the split form with the default, analytic and learned windows at TARGET")
     a = ap.parse_args()
     if a.evaluate:
         net = WindowMLP.load(a.out)
         for rec in evaluate(net, log2n=a.eval_log2n):
+            print(json.dumps(rec), flush=True)
+        return
+    if a.evaluate_split is not None:
+        net = WindowMLP.load(a.out)
+        for rec in evaluate_split(net, log2n=a.eval_log2n, target=a.evaluate_split):
             print(json.dumps(rec), flush=True)
         return
     if a.from_dataset:

@@ -86,24 +86,42 @@ def length_for(n_mu, d_mu, log2n):
 
 # ------------------------------------------------------------ measurement --
 
-def measure_error(x, S, n_mu, d_mu, B, tau, sigma, X=None):
-    """rel-L2 of the FP64 SOI transform of the CUDA complex128 tensor x against
-    the FP64 direct FFT X (computed when not given)."""
+def measure_error(x, S, n_mu, d_mu, B, tau, sigma, X=None, precision=PRECISION_FP64):
+    """rel-L2 of the SOI transform of the CUDA complex128 tensor x against the
+    FP64 direct FFT X (computed when not given), in the given precision form
+    (the split form transforms x rounded once to complex64)."""
     import torch
     if X is None:
         X = torch.fft.fft(x)
+    xin = x if precision == PRECISION_FP64 else x.to(torch.complex64)
     d = SoiDescriptor(N=x.numel(), n_mu=n_mu, d_mu=d_mu, B=B, tau=float(tau), sigma=float(sigma),
-                      precision=PRECISION_FP64, device=x.device.index or 0)
+                      precision=precision, device=x.device.index or 0)
     try:
         d.init(S)
-        y = torch.empty_like(x)
-        d.compute_into(x, y)
+        y = torch.empty_like(xin)
+        d.compute_into(xin, y)
     finally:
         d.free()
-    e = float(torch.linalg.norm(y - X) / torch.linalg.norm(X))
+    e = float(torch.linalg.norm(y.to(torch.complex128) - X) / torch.linalg.norm(X))
     if not math.isfinite(e):
         e = 1.0
     return e
+
+
+def conditioning(tau, sigma):
+    """max |W_inv| of the window: 1 / y_W(t) at the band edge |t| = 1/2, where
+    y_W(t) = (erfc(sqrt(sigma)(t - tau/2)) - erfc(sqrt(sigma)(t + tau/2))) / (2 tau)
+    (pfft.c:68-82) is smallest.  The demodulation multiplies by it, so it
+    amplifies the working precision's rounding: in the split form a window's
+    error is about its FP64 error plus SPLIT_ROUNDING * conditioning."""
+    sq = math.sqrt(sigma)
+    y = (math.erfc(sq * (0.5 - tau / 2)) - math.erfc(sq * (0.5 + tau / 2))) / (2 * tau)
+    return 1.0 / y if y > 0 else float("inf")
+
+
+# measured: the default window (conditioning 9.1) has split error 3.4e-7 and a
+# tau = 0.345, sigma = 56 window (conditioning ~1200) 5.2e-5 -> ~0.6 * 2^-24 each
+SPLIT_ROUNDING = 0.6 * 2.0 ** -24
 
 
 def sample_windows(rng, n, n_mu, d_mu):
@@ -232,12 +250,17 @@ class WindowMLP:
             out.append((int(b), float(taus[it]), float(sigs[isg]), float(pred[i, it, isg])))
         return out
 
-    def propose(self, n_mu, d_mu, target, slack=0.3, per_b=3):
-        """Candidates (B, tau, sigma, predicted log10 error) in increasing B: for
-        each B the `per_b` best-predicted (tau, sigma) whose prediction is
-        within `slack` decades of the target (the measurement decides)."""
+    def propose(self, n_mu, d_mu, target, slack=0.3, per_b=3, precision=PRECISION_FP64):
+        """Candidates (B, tau, sigma, predicted log10 error) in increasing B:
+        for each B the `per_b` best-predicted (tau, sigma) whose prediction is
+        within `slack` decades of the target (the measurement decides).  For the
+        split form the prediction is the FP64 one plus the window's
+        conditioning times the FP32 rounding."""
         lt = math.log10(target)
         Bs, taus, sigs, pred = self.predict_grid(n_mu, d_mu)
+        if precision != PRECISION_FP64:
+            cond = np.array([[conditioning(t, sg) for sg in sigs] for t in taus])
+            pred = np.log10(10.0 ** pred + SPLIT_ROUNDING * cond[None, :, :])
         out = []
         for i, b in enumerate(Bs):
             flat = pred[i].ravel()
@@ -263,10 +286,11 @@ def analytic_window(n_mu, d_mu, target, measure):
     return 72, 928 / 1024., 373.7314, e
 
 
-def learned_window(net, n_mu, d_mu, target, measure, tries=24):
+def learned_window(net, n_mu, d_mu, target, measure, tries=24, precision=PRECISION_FP64):
     """A verified proposal: the first candidate (smallest B) whose measured
-    error meets the target; None when none of the first `tries` does."""
-    for (B, tau, sigma, pred) in net.propose(n_mu, d_mu, target)[:tries]:
+    error (in `measure`'s precision form) meets the target; None when none of
+    the first `tries` does."""
+    for (B, tau, sigma, pred) in net.propose(n_mu, d_mu, target, precision=precision)[:tries]:
         e = measure(B, tau, sigma)
         if e <= target:
             return B, tau, sigma, e, pred
@@ -327,10 +351,10 @@ def evaluate(net, log2n=26, S=32, targets=(1e-12, 1e-11, 1e-10, 1e-9, 1e-8, 1e-7
 def evaluate_split(net, log2n=26, S=128, target=1e-6, seed=99, reps=5):
     """The split form at one accuracy target: the default window (B = 72), the
     analytic window and the learned window, each with its measured rel-L2 of the
-    split transform against the FP64 direct FFT and its median time.  The window
-    is chosen on the FP64 transform at target/4 (the split form adds ~3.5e-7 of
-    its own rounding), and accepted only if the split transform meets the
-    target.  Yields one dict per oversampling pair."""
+    split transform against the FP64 direct FFT and its median time.  Windows
+    are proposed with the split form's conditioning term and accepted only if
+    the split transform itself meets the target.  Yields one dict per
+    oversampling pair."""
     import torch
     from . import PRECISION_SPLIT_FP32
 
@@ -362,13 +386,17 @@ def evaluate_split(net, log2n=26, S=128, target=1e-6, seed=99, reps=5):
                           torch.randn(N, generator=g, device="cuda", dtype=torch.float64))
         X = torch.fft.fft(x)
         x32 = x.to(torch.complex64)
-        measure = lambda B, tau, sigma: measure_error(x, S, n_mu, d_mu, int(B), tau, sigma, X)
+        # windows are chosen and verified in the split form itself: a window that
+        # is accurate in FP64 can fail in FP32 when its demodulation is
+        # ill-conditioned
+        measure = lambda B, tau, sigma: measure_error(x, S, n_mu, d_mu, int(B), tau, sigma, X,
+                                                      precision=PRECISION_SPLIT_FP32)
         rec = {"mu": "%d/%d" % (n_mu, d_mu), "N": N, "S": S, "target": target}
         wins = {"default": (72, 928 / 1024., 373.7314)}
-        base = analytic_window(n_mu, d_mu, target / 4, measure)
-        if base[3] <= target / 4:
+        base = analytic_window(n_mu, d_mu, target, measure)
+        if base[3] <= target:
             wins["analytic"] = base[:3]
-        learned = learned_window(net, n_mu, d_mu, target / 4, measure)
+        learned = learned_window(net, n_mu, d_mu, target, measure, precision=PRECISION_SPLIT_FP32)
         if learned is not None:
             wins["learned"] = learned[:3]
         for name, (B, tau, sigma) in wins.items():

@@ -80,3 +80,20 @@ def test_learned_window_needs_fewer_taps_at_equal_accuracy(n_mu, d_mu, target):
         assert B <= base[0]
     print("mu=%d/%d target=%.0e learned B=%d (err %.2e, pred %.2e) analytic B=%d (err %.2e)"
           % (n_mu, d_mu, target, B, err, 10 ** pred, base[0], base[3]))
+
+
+@pytest.mark.parametrize("tau,sigma", [(928 / 1024., 373.7314), (0.3451, 56.26), (0.154, 73.21)])
+def test_split_error_follows_window_conditioning(tau, sigma):
+    # the split form's error is about the FP64 error plus the FP32 rounding
+    # amplified by max |W_inv| (the window's conditioning); proposals for the
+    # split form rely on this estimate, and verification decides
+    N, S = 1 << 22, 32
+    g = torch.Generator(device="cuda").manual_seed(5)
+    x = torch.complex(torch.randn(N, generator=g, device="cuda", dtype=torch.float64),
+                      torch.randn(N, generator=g, device="cuda", dtype=torch.float64))
+    X = torch.fft.fft(x)
+    B = 72
+    e64 = wm.measure_error(x, S, 5, 4, B, tau, sigma, X)
+    e32 = wm.measure_error(x, S, 5, 4, B, tau, sigma, X, precision=sb.PRECISION_SPLIT_FP32)
+    est = e64 + wm.SPLIT_ROUNDING * wm.conditioning(tau, sigma)
+    assert est / 4 <= e32 <= 4 * est, (e64, e32, est)

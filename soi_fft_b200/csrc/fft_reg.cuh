@@ -13,15 +13,15 @@
 namespace soi {
 
 // sizes with a twiddle table in constant memory, and their offsets
-constexpr int kRegSizes[] = { 2, 3, 4, 5, 6, 8, 10, 12, 15, 16, 20, 24, 30, 32, 40, 48, 60, 64 };
+constexpr int kRegSizes[] = { 2, 3, 4, 5, 6, 8, 9, 10, 12, 15, 16, 20, 24, 30, 32, 40, 48, 60, 64 };
 __host__ __device__ constexpr int reg_tw_offset(int F)
 {
   // cumulative sizes of kRegSizes (a table lookup is not usable in device code)
-  return F == 2 ? 0 : F == 3 ? 2 : F == 4 ? 5 : F == 5 ? 9 : F == 6 ? 14 : F == 8 ? 20 : F == 10 ? 28
-       : F == 12 ? 38 : F == 15 ? 50 : F == 16 ? 65 : F == 20 ? 81 : F == 24 ? 101 : F == 30 ? 125
-       : F == 32 ? 155 : F == 40 ? 187 : F == 48 ? 227 : F == 60 ? 275 : F == 64 ? 335 : -1;
+  return F == 2 ? 0 : F == 3 ? 2 : F == 4 ? 5 : F == 5 ? 9 : F == 6 ? 14 : F == 8 ? 20 : F == 9 ? 28
+       : F == 10 ? 37 : F == 12 ? 47 : F == 15 ? 59 : F == 16 ? 74 : F == 20 ? 90 : F == 24 ? 110
+       : F == 30 ? 134 : F == 32 ? 164 : F == 40 ? 196 : F == 48 ? 236 : F == 60 ? 284 : F == 64 ? 344 : -1;
 }
-constexpr int kRegTwTotal = 399;
+constexpr int kRegTwTotal = 408;
 
 // w_F^m = exp(-2 pi i m/F) at c_regtw[reg_tw_offset(F) + m]; filled by the
 // host (long double, rounded once) before the first launch.

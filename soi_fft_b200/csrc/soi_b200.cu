@@ -327,6 +327,10 @@ const S2ChoiceCT kS2CT[] = {
   SOI_S2CT(float, 10, 8, 8, 8, 8, 8),       // 640 x 512
   SOI_S2CT(float, 5, 8, 8, 8, 8, 8),        // 320 x 512
   SOI_S2CT(float, 5, 8, 8, 4, 8, 8),        // 320 x 256
+  SOI_S2CT(float, 8, 16, 16, 8, 16, 16),    // 2048 x 2048 (mu = 8/7: N = 7*2^26, S = 128)
+  SOI_S2CT(float, 9, 16, 16, 8, 16, 16),    // 2304 x 2048 (mu = 9/8: N = 2^29, S = 128)
+  SOI_S2CT(float, 8, 8, 8, 4, 16, 16),      // 512 x 1024  (mu = 8/7: N = 7*2^23, S = 128)
+  SOI_S2CT(float, 9, 8, 16, 8, 8, 8),       // 1152 x 512  (mu = 9/8: N = 2^26, S = 128)
   SOI_S2CT(double, 10, 16, 16, 8, 16, 16),
   SOI_S2CT(double, 10, 16, 16, 4, 16, 16),
   SOI_S2CT(double, 5, 16, 16, 4, 16, 16),
@@ -335,6 +339,10 @@ const S2ChoiceCT kS2CT[] = {
   SOI_S2CT(double, 10, 8, 8, 8, 8, 8),
   SOI_S2CT(double, 5, 8, 8, 8, 8, 8),
   SOI_S2CT(double, 5, 8, 8, 4, 8, 8),
+  SOI_S2CT(double, 8, 16, 16, 8, 16, 16),
+  SOI_S2CT(double, 9, 16, 16, 8, 16, 16),
+  SOI_S2CT(double, 8, 8, 8, 4, 16, 16),
+  SOI_S2CT(double, 9, 8, 16, 8, 8, 8),
 };
 #undef SOI_S2CT
 

@@ -246,6 +246,22 @@ def test_fast_paths_agree_with_fallback_kernels(prec, tol, N, S, monkeypatch):
     assert rel_l2(outs[0], outs[1]) <= tol
 
 
+@pytest.mark.parametrize("prec,tol", [(sb.PRECISION_FP64, 1e-13), (sb.PRECISION_SPLIT_FP32, 2e-6)])
+@pytest.mark.parametrize("N,S,n,d", [(7 << 23, 128, 8, 7), (1 << 26, 128, 9, 8)])
+def test_other_oversampling_persistent_stage2_agrees_with_fallback(prec, tol, N, S, n, d, monkeypatch):
+    # mu = 8/7 (M' = 512 x 1024) and 9/8 (M' = 1152 x 512, a radix-9 register
+    # stage) on the persistent stage 2, against the two-kernel stage 2
+    dt = np.complex128 if prec == sb.PRECISION_FP64 else np.complex64
+    x = on_gpu(signals.gaussian(N, 23, dt))
+    outs = []
+    for fast in ("1", "0"):
+        monkeypatch.setenv("SOI_STAGE2_FAST", fast)
+        desc = sb.SoiDescriptor(N=N, precision=prec, n_mu=n, d_mu=d).init(S)
+        outs.append(desc.compute(x.clone()).cpu().numpy().astype(np.complex128))
+        desc.free()
+    assert rel_l2(outs[0], outs[1]) <= tol
+
+
 def test_fp64_first_plan_in_a_fresh_process():
     # every plan must set up all device tables it uses: an FP64 plan made
     # first in a process (no split-form plan before it) must be exact

@@ -69,7 +69,10 @@ typedef struct {
   int precision;          /* soi_precision_t                                     */
   int device_ptr;         /* alpha_dt is a device pointer                        */
   int device;             /* CUDA device ordinal                                 */
-  void *stream;           /* cudaStream_t to run on (NULL: the library's own)    */
+  void *stream;           /* cudaStream_t to run on (NULL: the library's own,
+                             a blocking stream, ordered with the legacy
+                             default stream; with any other stream the caller
+                             orders the input's producer before the call)    */
   int last_status;        /* soi_status_t of the last call                       */
   void *plan;             /* opaque device state                                 */
 } soi_desc_t;

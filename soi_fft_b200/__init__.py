@@ -171,6 +171,13 @@ class SoiDescriptor:
             want = torch.complex128 if self._d.precision == PRECISION_FP64 else torch.complex64
             if x.dtype != want or not x.is_contiguous() or x.numel() != self._d.N:
                 raise ValueError("device array must be contiguous %s of length N" % want)
+            if not self._d.stream:
+                # the library's own stream is ordered with the legacy default
+                # stream only: work queued on a torch side stream (the tensor's
+                # producer) must finish before the library reads the tensor
+                cur = torch.cuda.current_stream(x.device)
+                if cur.cuda_stream != 0 and not torch.cuda.is_current_stream_capturing():
+                    cur.synchronize()
             self._d.device_ptr = 1
             return ctypes.c_void_p(x.data_ptr())
         if x.dtype != self._dtype() or not x.flags.c_contiguous or x.size != self._d.N:

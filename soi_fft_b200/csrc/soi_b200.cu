@@ -803,7 +803,12 @@ int make_plan(const soi_desc_t *d, size_t k, int knob_s1_nt, int knob_s2, bool w
   if (d->stream) {
     p->stream = (cudaStream_t)d->stream;
   } else {
-    if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess) { free_plan(p); return SOI_ERR_CUDA; }
+    // a blocking stream: it is ordered with the legacy default stream, so a
+    // device input written there (a copy, a producer kernel) is complete
+    // before stage 1 reads it, as the reference's synchronous compute_soi
+    // implies; a non-blocking stream let stage 1 read the circular halo at
+    // the end of an input that was still being written
+    if (cudaStreamCreate(&p->stream) != cudaSuccess) { free_plan(p); return SOI_ERR_CUDA; }
     p->own_stream = true;
   }
   for (auto &e : p->ev)

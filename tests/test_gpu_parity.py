@@ -268,6 +268,34 @@ def test_other_oversampling_persistent_stage2_agrees_with_fallback(prec, tol, N,
     assert rel_l2(outs[0], outs[1]) <= tol
 
 
+@pytest.mark.parametrize("side_stream", [False, True])
+def test_input_written_just_before_the_call_is_read_complete(side_stream):
+    # the input is filled by an asynchronous device copy queued right before
+    # the call (on torch's default stream, or on a side stream) over a buffer
+    # that held NaN; the library's own stream must not start stage 1 before the
+    # copy ends.  A first compute loads the kernels, so nothing delays the
+    # launches that follow.
+    N, S, prec = 1 << 26, 128, sb.PRECISION_SPLIT_FP32
+    x = on_gpu(signals.gaussian(N, 31, np.complex64))
+    X = torch.fft.fft(x.to(torch.complex128))
+    buf = torch.empty_like(x)
+    desc = sb.SoiDescriptor(N=N, precision=prec).init(S)
+    try:
+        desc.compute(x.clone())
+        s = torch.cuda.Stream() if side_stream else torch.cuda.current_stream()
+        for _ in range(3):
+            torch.view_as_real(buf).fill_(float("nan"))
+            torch.cuda.synchronize()
+            with torch.cuda.stream(s):
+                buf.copy_(x)
+                desc.compute(buf)
+            torch.cuda.synchronize()
+            e = float(torch.linalg.norm(buf.to(torch.complex128) - X) / torch.linalg.norm(X))
+            assert e <= 1e-6, e
+    finally:
+        desc.free()
+
+
 def test_fp64_first_plan_in_a_fresh_process():
     # every plan must set up all device tables it uses: an FP64 plan made
     # first in a process (no split-form plan before it) must be exact

@@ -54,6 +54,7 @@ struct Plan {
   // persistent stage 2: compiled radix split and its state
   int fast2 = 0;               // 0: two-kernel stage 2, 3: persistent kernel (4: chosen, not set up)
   int f2_variant = 0;
+  int f2_nt = 256;             // threads of the persistent stage-2 instance
   int f2_grid = 0;
   size_t f2_smem = 0;
   int discard = 1;             // drop consumed intermediate lines from L2
@@ -311,12 +312,17 @@ int upload_regtw()
 // ---- stage 2 with compile-time geometry ----------------------------------------
 
 using S2KernelCT = void (*)(S2ArgsCT);
-struct S2ChoiceCT { int M1, M2, elem, nt; size_t smem; S2KernelCT k; };
+struct S2ChoiceCT { int M1, M2, elem, nt, C; size_t smem; S2KernelCT k; };
 
-#define SOI_S2CT(R, a0, a1, a2, b0, b1, b2)                                                   \
-  { a0 * a1 * a2, b0 * b1 * b2, (int)sizeof(typename cplx_of<R>::type), 256,                 \
-    (size_t)S2Geom<R, a0, a1, a2, b0, b1, b2, 256>::BUF * S2Geom<R, a0, a1, a2, b0, b1, b2, 256>::E, \
-    k_stage2_ct<R, a0, a1, a2, b0, b1, b2, 256> }
+// one instance: pass-1 radices (a0, a1, a2), pass-2 radices (b0, b1, b2),
+// NT threads, C columns per task, at least MINB CTAs per SM (register bound)
+#define SOI_S2CTV(R, a0, a1, a2, b0, b1, b2, NT, C, MINB)                                         \
+  { a0 * a1 * a2, b0 * b1 * b2, (int)sizeof(typename cplx_of<R>::type), NT, C,                   \
+    (size_t)S2Geom<R, a0, a1, a2, b0, b1, b2, NT, C>::BUF * S2Geom<R, a0, a1, a2, b0, b1, b2, NT, C>::E, \
+    k_stage2_ct<R, a0, a1, a2, b0, b1, b2, NT, C, MINB> }
+// the default instance: 256 threads, a whole 32-byte sector per row run, two CTAs per SM
+#define SOI_S2CT(R, a0, a1, a2, b0, b1, b2) \
+  SOI_S2CTV(R, a0, a1, a2, b0, b1, b2, 256, 32 / (int)sizeof(typename cplx_of<R>::type), 2)
 
 const S2ChoiceCT kS2CT[] = {
   SOI_S2CT(float, 10, 16, 16, 8, 16, 16),   // M' = 2560 x 2048 (N = 2^29, S = 128; 2^28, 64)
@@ -345,6 +351,7 @@ const S2ChoiceCT kS2CT[] = {
   SOI_S2CT(double, 9, 8, 16, 8, 8, 8),
 };
 #undef SOI_S2CT
+#undef SOI_S2CTV
 
 // index into kS2CT for M' and the element size, or -1
 int pick_s2ct(const Plan &p)
@@ -402,7 +409,8 @@ int setup_s2ct(Plan &p, int idx)
 {
   const S2ChoiceCT &c = kS2CT[idx];
   p.M1 = c.M1; p.M2 = c.M2;
-  p.C1 = p.C2 = 32 / c.elem;
+  p.C1 = p.C2 = c.C;
+  p.f2_nt = c.nt;
   p.f2_smem = c.smem;
   p.f2ct_kernel = c.k;
   CK(cudaFuncSetAttribute(c.k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.f2_smem));
@@ -434,7 +442,7 @@ int launch_s2ct(Plan &p, const Exec &ex)
   a.err = (int *)ex.sync; a.counter = ex.sync + 1; a.done1 = ex.sync + 2;
   // counters restart; the error flag stays set until the owner clears it
   CK(cudaMemsetAsync(ex.sync + 1, 0, (size_t)(a.S + 1) * sizeof(unsigned int), ex.st));
-  p.f2ct_kernel<<<p.f2_grid, 256, p.f2_smem, ex.st>>>(a);
+  p.f2ct_kernel<<<p.f2_grid, p.f2_nt, p.f2_smem, ex.st>>>(a);
   CK(cudaGetLastError());
   return SOI_OK;
 }
@@ -761,7 +769,7 @@ int plan_geometry(const soi_desc_t *d, size_t k, Plan &p)
     p.f2_variant = ict;
     p.M1 = kS2CT[ict].M1;
     p.M2 = kS2CT[ict].M2;
-    p.C1 = p.C2 = 32 / kS2CT[ict].elem;
+    p.C1 = p.C2 = kS2CT[ict].C;
     p.fast2 = 4;                 // chosen; set up when the device plan is built
     make_fft_plan(p.M1, p.plan1);
     make_fft_plan(p.M2, p.plan2);

@@ -125,7 +125,7 @@ template <typename V, int C1, int M2, int RL> struct EmitColsCT {
 
 struct NoPre {};
 
-template <typename V, int M1, int RL> struct EmitRowsCT {
+template <typename V, int M1, int RL, bool BATCH> struct EmitRowsCT {
   V *oseg; int k1_0; const V *ph1; const S2ArgsCT *a;
   __device__ __forceinline__ NoPre prepare(int, int) const { return NoPre{}; }
   template <int RLx> __device__ __forceinline__ void run(int col, int fbase, int fstep, V *v, NoPre) const
@@ -139,8 +139,9 @@ template <typename V, int M1, int RL> struct EmitRowsCT {
     const Rr *amp = reinterpret_cast<const Rr *>(a->amp);
     // every load in bounds (discarded bins read amp[0]), so the loads do not
     // wait on the discard test
-    if constexpr (sizeof(V) == 8) {
-      // FP32: all RL factors in flight before the first store
+    if constexpr (sizeof(V) == 8 && BATCH) {
+      // FP32 with registers to spare: all RL factors in flight before the
+      // first store
       V w[RL];
 #pragma unroll
       for (int j = 0; j < RL; ++j) {
@@ -155,7 +156,8 @@ template <typename V, int M1, int RL> struct EmitRowsCT {
         if (k < M) stcs(oseg + k, cmul(v[j], w[j]));
       }
     } else {
-      // FP64: RL double factors would not fit in registers beside the data
+      // FP64, or a tight register budget: RL factors would not fit beside
+      // the data
 #pragma unroll
       for (int j = 0; j < RL; ++j) {
         const int k2 = fbase + fstep * j;
@@ -175,27 +177,30 @@ template <int base, int mod, int rem> constexpr int round_up_to_residue()
   return x;
 }
 
-template <typename R, int A0, int A1, int A2, int B0, int B1, int B2, int NT>
+template <typename R, int A0, int A1, int A2, int B0, int B1, int B2, int NT, int CC>
 struct S2Geom {
   using V = typename cplx_of<R>::type;
   static constexpr int E = (int)sizeof(V);
-  static constexpr int C = 32 / E;                          // columns (rows) per task
+  static constexpr int C = CC;                              // columns (rows) per task
+  static_assert(C * E == 32 || C * E == 16, "a task's row run is a whole or a half 32-byte sector");
+  static constexpr int CPR1 = C * E / 16;                   // 16-byte chunks per pass-1 row run
   static constexpr int M1 = A0 * A1 * A2, M2 = B0 * B1 * B2;
   static constexpr int RLA = A2 > 1 ? A2 : A1, RLB = B2 > 1 ? B2 : B1;
   static constexpr int NT1 = M2 / C, NT2 = M1 / C, PER = NT1 + NT2;
-  // pass-2 row pitch: the C rows land on disjoint banks in the last stage
-  // (8-byte elements: pitch = 4 mod 16; 16-byte elements: pitch = 4 mod 8)
-  static constexpr int PS2 = E == 8 ? round_up_to_residue<M2 + M2 / RLB, 16, 4>()
-                                    : round_up_to_residue<M2 + M2 / RLB, 8, 4>();
+  // pass-2 row pitch: the C rows land on disjoint banks in the last stage,
+  // whose loads the hardware splits into groups of 128 bytes (16 eight-byte
+  // or 8 sixteen-byte slots): pitch = (slots / C) mod slots
+  static constexpr int SLOTS = 128 / E;
+  static constexpr int PS2 = round_up_to_residue<M2 + M2 / RLB, SLOTS, (SLOTS / C) % SLOTS>();
   static constexpr int BUF1 = (M1 + M1 / RLA) * C, BUF2 = PS2 * C;
   static constexpr int BUF = BUF1 > BUF2 ? BUF1 : BUF2;
   static constexpr int TAB = C * RLA;                       // shared table entries
 };
 
-template <typename R, int A0, int A1, int A2, int B0, int B1, int B2, int NT>
-__global__ void __launch_bounds__(NT, 2) k_stage2_ct(S2ArgsCT a)
+template <typename R, int A0, int A1, int A2, int B0, int B1, int B2, int NT, int CC, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_stage2_ct(S2ArgsCT a)
 {
-  using G = S2Geom<R, A0, A1, A2, B0, B1, B2, NT>;
+  using G = S2Geom<R, A0, A1, A2, B0, B1, B2, NT, CC>;
   using V = typename G::V;
   constexpr int C = G::C, M1 = G::M1, M2 = G::M2, RLA = G::RLA, RLB = G::RLB;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -205,6 +210,14 @@ __global__ void __launch_bounds__(NT, 2) k_stage2_ct(S2ArgsCT a)
   __shared__ int s_ok[2];
   const int tid = threadIdx.x;
   const unsigned int total = (unsigned int)a.S * G::PER;
+  // task index -> (pass, segment, tile) in the order P1(0), P1(1), P2(0), P1(2), ...
+  auto decode = [&](unsigned int t, int &kind, int &seg, int &tile) {
+    if (t < (unsigned int)G::NT1) { kind = 1; seg = 0; tile = (int)t; return; }
+    const unsigned int u = t - G::NT1;
+    const int blk = (int)(u / G::PER), r = (int)(u % G::PER);
+    if (blk < a.S - 1 && r < G::NT1) { kind = 1; seg = blk + 1; tile = r; }
+    else { kind = 2; seg = blk; tile = r - (blk < a.S - 1 ? G::NT1 : 0); }
+  };
   unsigned int next = 0;
   // thread 0: take the claimed task, claim the one after it, and for a
   // pass-2 task wait (bounded) until its segment's pass 1 is complete; the
@@ -214,12 +227,12 @@ __global__ void __launch_bounds__(NT, 2) k_stage2_ct(S2ArgsCT a)
     if (t < total) next = atomicAdd(a.counter, 1u);
     if (*(volatile int *)a.err) t = total;
     int ok = 1;
-    if (t < total && t >= (unsigned int)G::NT1) {
-      const unsigned int u = t - G::NT1;
-      const int blk = (int)(u / G::PER), r = (int)(u % G::PER);
-      if (blk >= a.S - 1 || r >= G::NT1) {                  // pass-2 task of segment blk
+    if (t < total) {
+      int kind, seg, tile;
+      decode(t, kind, seg, tile);
+      if (kind == 2) {                                      // pass-2 task of segment seg
         long long it = 0;
-        while (ld_acquire_u32(a.done1 + blk) < (unsigned int)(G::NT1 + a.wait_extra)) {
+        while (ld_acquire_u32(a.done1 + seg) < (unsigned int)(G::NT1 + a.wait_extra)) {
           if (++it > kWaitLimit) { atomicExch(a.err, 1); ok = 0; break; }
           if (*(volatile int *)a.err) { ok = 0; break; }   // another CTA gave up
           __nanosleep(128);
@@ -240,20 +253,15 @@ __global__ void __launch_bounds__(NT, 2) k_stage2_ct(S2ArgsCT a)
     const unsigned int t = s_task[slot];
     if (t >= total || !s_ok[slot]) break;
     int kind, seg, tile;
-    if (t < (unsigned int)G::NT1) { kind = 1; seg = 0; tile = (int)t; }
-    else {
-      const unsigned int u = t - G::NT1;
-      const int blk = (int)(u / G::PER), r = (int)(u % G::PER);
-      if (blk < a.S - 1 && r < G::NT1) { kind = 1; seg = blk + 1; tile = r; }
-      else { kind = 2; seg = blk; tile = r - (blk < a.S - 1 ? G::NT1 : 0); }
-    }
+    decode(t, kind, seg, tile);
     V *Tseg = reinterpret_cast<V *>(a.T) + (size_t)(a.seg_lo + seg) * ((size_t)M1 * M2);
     if (kind == 1) {
       const int m2_0 = tile * C;
-      // rows m1 of C columns: 32 bytes = 2 chunks of 16
+      // rows m1 of C columns: CPR1 chunks of 16 bytes each
       constexpr int EPC = 16 / G::E;                        // elements per 16-byte chunk
-      for (int q = tid; q < M1 * 2; q += NT) {
-        const int row = q >> 1, h = q & 1;
+      constexpr int CPR1 = G::CPR1;
+      for (int q = tid; q < M1 * CPR1; q += NT) {
+        const int row = q / CPR1, h = q % CPR1;
         cp_async_16cg(buf + (row + row / RLA) * C + h * EPC, Tseg + row * M2 + m2_0 + h * EPC);
       }
       cp_commit();
@@ -295,7 +303,7 @@ __global__ void __launch_bounds__(NT, 2) k_stage2_ct(S2ArgsCT a)
         constexpr int nlines = C * M2 * G::E / 128;
         for (int l = tid; l < nlines; l += NT) discard_l2_line(base + l * 128);
       }
-      EmitRowsCT<V, M1, RLB> e{ reinterpret_cast<V *>(a.out) + (size_t)(a.seg_lo + seg) * a.M, k1_0, s_tab, &a };
+      EmitRowsCT<V, M1, RLB, (MINB <= 2)> e{ reinterpret_cast<V *>(a.out) + (size_t)(a.seg_lo + seg) * a.M, k1_0, s_tab, &a };
       tile_fft_ct<V, B0, B1, B2, C, 1, G::PS2, NT>(buf, reinterpret_cast<const V *>(a.tw2), e);
       if (tid == 0) take(slot ^ 1);                           // after thread 0's own stores
     }

@@ -178,7 +178,7 @@ __device__ __forceinline__ void tile_fft_ct(V *sm, const V *__restrict__ tw, con
       RegDFT<V, R0>::run(v);
       p[0] = v[0];
 #pragma unroll
-      for (int k = 1; k < R0; ++k) p[k * D0] = cmul(v[k], __ldg(tw + i * k));
+      for (int k = 1; k < R0; ++k) p[k * D0] = cmul(v[k], __ldg(tw + (k - 1) * span0 + i));
     }
   }
   __syncthreads();
@@ -196,7 +196,7 @@ __device__ __forceinline__ void tile_fft_ct(V *sm, const V *__restrict__ tw, con
       RegDFT<V, R1>::run(v);
       p[0] = v[0];
 #pragma unroll
-      for (int k = 1; k < R1; ++k) p[k * DL] = cmul(v[k], __ldg(tw + i * k * R0));
+      for (int k = 1; k < R1; ++k) p[k * DL] = cmul(v[k], __ldg(tw + (R0 - 1) * span0 + (k - 1) * span1 + i));
     }
     __syncthreads();
   }
@@ -215,7 +215,7 @@ __device__ __forceinline__ void tile_fft_ct(V *sm, const V *__restrict__ tw, con
 #pragma unroll
       for (int r = 0; r < RL; ++r) v[r] = p[r * PP];
       RegDFT<V, RL>::run(v);
-      emit.template run<RL>(col, fbase, L / RL, v, pre);
+      emit.template run<RL>(col, fbase, L / RL, v, pre, blk);
     }
   }
 }

@@ -59,11 +59,12 @@ struct Plan {
   size_t f2_smem = 0;
   int discard = 1;             // drop consumed intermediate lines from L2
   int wait_extra = 0;          // failure test: pass-2 waits for a count that never comes
-  void *d_amp = nullptr;            // [M/2+1] real demodulation amplitude
+  void *d_amp = nullptr;            // [M1][M2] real demodulation amplitude, pass-2 store order
+  void *d_ctw1 = nullptr, *d_ctw2 = nullptr;   // tile-FFT twiddles of the two passes, warp read order
   double2 *d_dlo = nullptr, *d_dhi = nullptr;
   int dlo_bits = 11;
   void (*f2ct_kernel)(S2ArgsCT) = nullptr;
-  void *d_ph2 = nullptr;            // [M2] complex exp(-i pi kappa M1 k2 / M)
+  void *d_ph2 = nullptr;            // [M2] complex exp(-i pi kappa M1 k2 / M), pass-2 store order
   unsigned int *d_sync = nullptr;   // [0] err, [1] counter, [2..2+S) done1
   // staged stage 1
   int s1fast = 0, JR2 = 0, JT2 = 0, AC = 0, buf_elems = 0;
@@ -312,12 +313,12 @@ int upload_regtw()
 // ---- stage 2 with compile-time geometry ----------------------------------------
 
 using S2KernelCT = void (*)(S2ArgsCT);
-struct S2ChoiceCT { int M1, M2, elem, nt, C; size_t smem; S2KernelCT k; };
+struct S2ChoiceCT { int M1, M2, elem, nt, C; int ra[3], rb[3]; size_t smem; S2KernelCT k; };
 
 // one instance: pass-1 radices (a0, a1, a2), pass-2 radices (b0, b1, b2),
 // NT threads, C columns per task, at least MINB CTAs per SM (register bound)
 #define SOI_S2CTV(R, a0, a1, a2, b0, b1, b2, NT, C, MINB)                                         \
-  { a0 * a1 * a2, b0 * b1 * b2, (int)sizeof(typename cplx_of<R>::type), NT, C,                   \
+  { a0 * a1 * a2, b0 * b1 * b2, (int)sizeof(typename cplx_of<R>::type), NT, C, { a0, a1, a2 }, { b0, b1, b2 }, \
     (size_t)S2Geom<R, a0, a1, a2, b0, b1, b2, NT, C>::BUF * S2Geom<R, a0, a1, a2, b0, b1, b2, NT, C>::E, \
     k_stage2_ct<R, a0, a1, a2, b0, b1, b2, NT, C, MINB> }
 // the default instance: 256 threads, a whole 32-byte sector per row run, two CTAs per SM
@@ -363,11 +364,49 @@ int pick_s2ct(const Plan &p)
   return -1;
 }
 
-// demodulation tables shared by both persistent kernels: amp[k] = 1/y_W(k/M - 1/2)
-// for k <= M/2 (even about M/2), exp(-i pi kappa k/M) two-level in FP64, and
-// (compile-time kernel) ph2[k2] = exp(-i pi kappa M1 k2/M)
+// Twiddles of a tile FFT with radices (r0, r1, r2) over L = r0*r1*r2 points,
+// in the order the warps read them (8 consecutive butterflies of a warp read
+// 8 consecutive entries, one cache line): first stage w_L^(i*k) at
+// [(k-1)*span0 + i], span0 = L/r0; second stage (r2 > 1) w_L^(i*k*r0) at
+// [(r0-1)*span0 + (k-1)*r2 + i].  Same values as roots_table(L).
 template <typename R>
-int build_demod_tables(Plan &p, bool with_ph2)
+std::vector<R> tile_twiddles(int r0, int r1, int r2)
+{
+  const long long L = (long long)r0 * r1 * r2, span0 = L / r0;
+  std::vector<R> t;
+  auto push = [&](long long m) {
+    long double a = -2.0L * kPi * (long double)m / (long double)L;
+    t.push_back((R)cosl(a));
+    t.push_back((R)sinl(a));
+  };
+  for (int k = 1; k < r0; ++k)
+    for (long long i = 0; i < span0; ++i) push(i * k);
+  if (r2 > 1)
+    for (int k = 1; k < r1; ++k)
+      for (long long i = 0; i < r2; ++i) push(i * k * r0);
+  return t;
+}
+
+// Output k2 of pass 2's last radix stage at store position pos = blk + nb*j
+// (butterfly blk of nb = M2/RL, its output j), for radices (b0, b1, b2).
+inline long long pass2_k2(const int *rb, long long pos)
+{
+  const long long M2 = (long long)rb[0] * rb[1] * rb[2];
+  const long long RL = rb[2] > 1 ? rb[2] : rb[1], nb = M2 / RL;
+  const long long blk = pos % nb, j = pos / nb;
+  const long long fbase = rb[2] > 1 ? blk / rb[1] + rb[0] * (blk % rb[1]) : blk;
+  return fbase + nb * j;
+}
+
+// Tables of the persistent stage 2.  Demodulation: amp(k) = 1/y_W(k/M - 1/2)
+// (even about M/2) and exp(-i pi kappa k/M) = ph(k1) * ph(M1*k2), ph(k1) two-level
+// in FP64, ph(M1*k2) per k2.  amp and ph(M1*k2) are stored in the order pass 2's
+// last radix stores its outputs: for the task of rows k1 = C*t .. C*t + C-1,
+// amp[(t*M2 + pos)*C + col] is amp at k = C*t + col + M1*k2(pos), and
+// ph2[pos] is ph(M1*k2(pos)), so that a warp's loads are one cache line each.
+// Tile twiddles of both passes in warp read order (tile_twiddles).
+template <typename R>
+int build_ct_tables(Plan &p, const S2ChoiceCT &c)
 {
   const size_t M = p.M, half = M / 2 + 1;
   const long double sq = sqrtl((long double)p.sigma);
@@ -377,8 +416,19 @@ int build_demod_tables(Plan &p, bool with_ph2)
     long double y = (erfcl(sq * (t - p.tau / 2.0L)) - erfcl(sq * (t + p.tau / 2.0L))) / (2.0L * p.tau);
     af[i] = (R)(1.0L / y);
   }
+  const long long M1 = c.M1, M2 = c.M2, C = c.C;
+  std::vector<long long> k2of(M2);
+  for (long long pos = 0; pos < M2; ++pos) k2of[pos] = pass2_k2(c.rb, pos);
+  std::vector<R> amp((size_t)M1 * M2);
+  for (long long t = 0; t < M1 / C; ++t)
+    for (long long pos = 0; pos < M2; ++pos)
+      for (long long col = 0; col < C; ++col) {
+        const long long k = C * t + col + M1 * k2of[pos];
+        const long long km = k >= (long long)M ? 0 : std::min(k, (long long)M - k);
+        amp[(size_t)((t * M2 + pos) * C + col)] = af[(size_t)km];
+      }
   int rc;
-  if ((rc = upload(&p.d_amp, af.data(), af.size() * sizeof(R)))) return rc;
+  if ((rc = upload(&p.d_amp, amp.data(), amp.size() * sizeof(R)))) return rc;
   const long long kappa = (long long)p.B - p.dmu;
   auto phase = [&](long long k, long double *o) {
     long long q = (long long)(((unsigned long long)kappa * (unsigned long long)k) % (2ULL * M));
@@ -393,15 +443,16 @@ int build_demod_tables(Plan &p, bool with_ph2)
   for (long long h = 0; h < nhi; ++h) { phase(h * nlo, o); hi[2 * h] = (double)o[0]; hi[2 * h + 1] = (double)o[1]; }
   if ((rc = upload((void **)&p.d_dlo, lo.data(), lo.size() * sizeof(double)))) return rc;
   if ((rc = upload((void **)&p.d_dhi, hi.data(), hi.size() * sizeof(double)))) return rc;
-  if (with_ph2) {
-    std::vector<R> ph(2 * (size_t)p.M2);
-    for (int k2 = 0; k2 < p.M2; ++k2) {
-      phase((long long)p.M1 * k2, o);
-      ph[2 * k2] = (R)o[0];
-      ph[2 * k2 + 1] = (R)o[1];
-    }
-    if ((rc = upload(&p.d_ph2, ph.data(), ph.size() * sizeof(R)))) return rc;
+  std::vector<R> ph(2 * (size_t)M2);
+  for (long long pos = 0; pos < M2; ++pos) {
+    phase(M1 * k2of[pos], o);
+    ph[2 * pos] = (R)o[0];
+    ph[2 * pos + 1] = (R)o[1];
   }
+  if ((rc = upload(&p.d_ph2, ph.data(), ph.size() * sizeof(R)))) return rc;
+  std::vector<R> w1 = tile_twiddles<R>(c.ra[0], c.ra[1], c.ra[2]), w2 = tile_twiddles<R>(c.rb[0], c.rb[1], c.rb[2]);
+  if ((rc = upload(&p.d_ctw1, w1.data(), w1.size() * sizeof(R)))) return rc;
+  if ((rc = upload(&p.d_ctw2, w2.data(), w2.size() * sizeof(R)))) return rc;
   return SOI_OK;
 }
 
@@ -419,7 +470,7 @@ int setup_s2ct(Plan &p, int idx)
   CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, p.device));
   if (occ < 1) return SOI_ERR_UNSUPPORTED;
   p.f2_grid = occ * nsm;
-  int rc = p.prec == SOI_PRECISION_FP64 ? build_demod_tables<double>(p, true) : build_demod_tables<float>(p, true);
+  int rc = p.prec == SOI_PRECISION_FP64 ? build_ct_tables<double>(p, c) : build_ct_tables<float>(p, c);
   if (rc) return rc;
   p.discard = env_int("SOI_STAGE2_DISCARD", 1);
   // failure-detection test only: every pass-2 task then waits for one more
@@ -433,7 +484,7 @@ int setup_s2ct(Plan &p, int idx)
 int launch_s2ct(Plan &p, const Exec &ex)
 {
   S2ArgsCT a;
-  a.T = ex.T; a.out = ex.out; a.tw1 = p.d_tw1; a.tw2 = p.d_tw2; a.xlo = p.d_xlo; a.xhi = p.d_xhi;
+  a.T = ex.T; a.out = ex.out; a.tw1 = p.d_ctw1; a.tw2 = p.d_ctw2; a.xlo = p.d_xlo; a.xhi = p.d_xhi;
   a.amp = p.d_amp; a.dlo = p.d_dlo; a.dhi = p.d_dhi; a.ph2 = p.d_ph2;
   a.lo_bits = p.lo_bits; a.dlo_bits = p.dlo_bits; a.M = (int)p.M;
   a.S = ex.hi - ex.lo; a.seg_lo = ex.lo;
@@ -727,7 +778,7 @@ void free_plan(Plan *p)
   cudaSetDevice(p->device);
   void *bufs[] = { p->d_filt, p->d_phase, p->d_twS, p->d_tw1, p->d_tw2, p->d_winv, p->d_wsmall,
                    p->d_permS, p->d_perm1, p->d_perm2, p->d_xlo, p->d_xhi, p->d_T, p->d_io, p->d_io2,
-                   p->d_vlc_words, p->d_vlc_n, p->d_vlc_emax, p->d_sync, p->d_filt2, p->d_amp, p->d_dlo, p->d_dhi, p->d_ph2 };
+                   p->d_vlc_words, p->d_vlc_n, p->d_vlc_emax, p->d_sync, p->d_filt2, p->d_amp, p->d_dlo, p->d_dhi, p->d_ph2, p->d_ctw1, p->d_ctw2 };
   for (void *b : bufs) if (b) cudaFree(b);
   for (auto &e : p->ev) if (e) cudaEventDestroy(e);
   for (auto &e : p->sev) if (e) cudaEventDestroy(e);
@@ -906,7 +957,7 @@ int compute_impl(soi_desc_t *d, const void *in, void *out, bool stage1_only, int
 int vlc_alloc(Plan &p)
 {
   if (p.d_vlc_words) return SOI_OK;
-  const size_t S = p.S, len = 2 * p.Mh;
+  const size_t S = p.S;
   p.vlc_stride = (long)(4 * p.Mh + 64);
   CK(cudaMalloc(&p.d_vlc_words, (size_t)p.vlc_stride * S * sizeof(int)));
   CK(cudaMalloc(&p.d_vlc_n, S * sizeof(int)));

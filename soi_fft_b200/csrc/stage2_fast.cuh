@@ -21,9 +21,12 @@
 // step[col][k] = w_{M'}^(m2*fstep*k), the C x RL step table built per task in
 // shared memory.  Pass 2: W_inv[k], k = k1 + M1*k2, is
 // amp[min(k, M-k)] * ph(k1) * ph(M1*k2) with ph(k) = exp(-i pi kappa k/M);
-// ph(k1) per task in shared memory, ph(M1*k2) from an M2-entry table.  Every
-// table entry is FP64-generated and rounded once; the products are formed in
-// the working precision.
+// ph(k1) per task in shared memory, amp and ph(M1*k2) from tables laid out in
+// the order the last radix stage stores its outputs, and the tile twiddles
+// from tables in the order the radix stages read them, so that every table
+// load of a warp is one cache line (the SM's load/store data path is this
+// kernel's busiest unit).  Every table entry is FP64-generated and rounded
+// once; the products are formed in the working precision.
 //
 // Schedule: CTAs take tasks from a global counter in the order
 //   P1(0), P1(1), P2(0), P1(2), P2(1), ..., P2(S-1),
@@ -82,11 +85,11 @@ __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_grou
 struct S2ArgsCT {
   void *T;                    // [S][Mh] pass-1 input, intermediate in place
   void *out;                  // [S][M]
-  const void *tw1, *tw2;      // exp(-2 pi i m/M1), exp(-2 pi i m/M2)
+  const void *tw1, *tw2;      // tile twiddles of the two passes, warp read order
   const double2 *xlo, *xhi;   // w_{M'}^e two-level, FP64
-  const void *amp;            // [M/2 + 1] real
+  const void *amp;            // [M1][M2] real, pass-2 store order per task
   const double2 *dlo, *dhi;   // exp(-i pi kappa k/M) two-level, FP64
-  const void *ph2;            // [M2] complex: exp(-i pi kappa M1 k2 / M)
+  const void *ph2;            // [M2] complex exp(-i pi kappa M1 k2 / M), pass-2 store order
   int lo_bits, dlo_bits;
   int M;
   int S;                      // segments in this launch
@@ -112,7 +115,7 @@ template <typename V, int C1, int M2, int RL> struct EmitColsCT {
   {
     return two_level<V>(a->xlo, a->xhi, a->lo_bits, (m2_0 + col) * fbase);
   }
-  template <int RLx> __device__ __forceinline__ void run(int col, int fbase, int fstep, V *v, V base) const
+  template <int RLx> __device__ __forceinline__ void run(int col, int fbase, int fstep, V *v, V base, int) const
   {
     static_assert(RLx == RL, "last radix");
     const int m2 = m2_0 + col;
@@ -125,10 +128,14 @@ template <typename V, int C1, int M2, int RL> struct EmitColsCT {
 
 struct NoPre {};
 
-template <typename V, int M1, int RL, bool BATCH> struct EmitRowsCT {
+// amp and ph(M1*k2) come from tables in this stage's store order: output j of
+// butterfly blk is position pos = blk + fstep*j, and the task's rows k1_0 ..
+// k1_0 + C-1 own amp[(k1_0*M2 + pos*C) + col], so that a warp's loads (8
+// consecutive butterflies x C rows) are one cache line each
+template <typename V, int M1, int M2, int C, int RL, bool BATCH> struct EmitRowsCT {
   V *oseg; int k1_0; const V *ph1; const S2ArgsCT *a;
   __device__ __forceinline__ NoPre prepare(int, int) const { return NoPre{}; }
-  template <int RLx> __device__ __forceinline__ void run(int col, int fbase, int fstep, V *v, NoPre) const
+  template <int RLx> __device__ __forceinline__ void run(int col, int fbase, int fstep, V *v, NoPre, int blk) const
   {
     static_assert(RLx == RL, "last radix");
     using Rr = decltype(V::x);
@@ -136,19 +143,15 @@ template <typename V, int M1, int RL, bool BATCH> struct EmitRowsCT {
     const int M = a->M;
     const V p1 = ph1[col];
     const V *ph2 = reinterpret_cast<const V *>(a->ph2);
-    const Rr *amp = reinterpret_cast<const Rr *>(a->amp);
-    // every load in bounds (discarded bins read amp[0]), so the loads do not
-    // wait on the discard test
+    const Rr *amp = reinterpret_cast<const Rr *>(a->amp) + (size_t)k1_0 * M2 + col;
     if constexpr (sizeof(V) == 8 && BATCH) {
       // FP32 with registers to spare: all RL factors in flight before the
       // first store
       V w[RL];
 #pragma unroll
       for (int j = 0; j < RL; ++j) {
-        const int k2 = fbase + fstep * j;
-        const int k = k1 + M1 * k2;
-        const int km = k >= M ? 0 : (k <= M - k ? k : M - k);
-        w[j] = cscale(cmul(p1, __ldg(ph2 + k2)), __ldg(amp + km));
+        const int pos = blk + fstep * j;
+        w[j] = cscale(cmul(p1, __ldg(ph2 + pos)), __ldg(amp + pos * C));
       }
 #pragma unroll
       for (int j = 0; j < RL; ++j) {
@@ -160,10 +163,9 @@ template <typename V, int M1, int RL, bool BATCH> struct EmitRowsCT {
       // the data
 #pragma unroll
       for (int j = 0; j < RL; ++j) {
-        const int k2 = fbase + fstep * j;
-        const int k = k1 + M1 * k2;
-        const int km = k >= M ? 0 : (k <= M - k ? k : M - k);
-        const V w = cscale(cmul(p1, __ldg(ph2 + k2)), __ldg(amp + km));
+        const int pos = blk + fstep * j;
+        const int k = k1 + M1 * (fbase + fstep * j);
+        const V w = cscale(cmul(p1, __ldg(ph2 + pos)), __ldg(amp + pos * C));
         if (k < M) stcs(oseg + k, cmul(v[j], w));
       }
     }
@@ -303,7 +305,7 @@ __global__ void __launch_bounds__(NT, MINB) k_stage2_ct(S2ArgsCT a)
         constexpr int nlines = C * M2 * G::E / 128;
         for (int l = tid; l < nlines; l += NT) discard_l2_line(base + l * 128);
       }
-      EmitRowsCT<V, M1, RLB, (MINB <= 2)> e{ reinterpret_cast<V *>(a.out) + (size_t)(a.seg_lo + seg) * a.M, k1_0, s_tab, &a };
+      EmitRowsCT<V, M1, M2, C, RLB, (MINB <= 2)> e{ reinterpret_cast<V *>(a.out) + (size_t)(a.seg_lo + seg) * a.M, k1_0, s_tab, &a };
       tile_fft_ct<V, B0, B1, B2, C, 1, G::PS2, NT>(buf, reinterpret_cast<const V *>(a.tw2), e);
       if (tid == 0) take(slot ^ 1);                           // after thread 0's own stores
     }

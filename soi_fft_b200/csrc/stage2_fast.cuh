@@ -19,7 +19,7 @@
 // Epilogue factors come from per-task tables instead of scattered lookups.
 // Pass 1: w_{M'}^(m2*f) for f = fbase + fstep*k is base(m2*fbase) times
 // step[col][k] = w_{M'}^(m2*fstep*k), the C x RL step table built per task in
-// shared memory.  Pass 2: W_inv[k], k = k1 + M1*k2, is
+// shared memory (row pitch RL + 1).  Pass 2: W_inv[k], k = k1 + M1*k2, is
 // amp[min(k, M-k)] * ph(k1) * ph(M1*k2) with ph(k) = exp(-i pi kappa k/M);
 // ph(k1) per task in shared memory, amp and ph(M1*k2) from tables laid out in
 // the order the last radix stage stores its outputs, and the tile twiddles
@@ -122,7 +122,7 @@ template <typename V, int C1, int M2, int RL> struct EmitColsCT {
     V *dst = Tseg + fbase * M2 + m2;
     dst[0] = cmul(v[0], base);
 #pragma unroll
-    for (int k = 1; k < RL; ++k) dst[k * fstep * M2] = cmul(v[k], cmul(base, step[col * RL + k]));
+    for (int k = 1; k < RL; ++k) dst[k * fstep * M2] = cmul(v[k], cmul(base, step[col * (RL + 1) + k]));
   }
 };
 
@@ -196,7 +196,10 @@ struct S2Geom {
   static constexpr int PS2 = round_up_to_residue<M2 + M2 / RLB, SLOTS, (SLOTS / C) % SLOTS>();
   static constexpr int BUF1 = (M1 + M1 / RLA) * C, BUF2 = PS2 * C;
   static constexpr int BUF = BUF1 > BUF2 ? BUF1 : BUF2;
-  static constexpr int TAB = C * RLA;                       // shared table entries
+  // shared table entries: the pass-1 step table, one row of RLA + 1 per
+  // column (the pad puts a warp's C columns on different banks; at a pitch of
+  // RLA every read of the table was a C-way bank conflict)
+  static constexpr int TAB = C * (RLA + 1);
 };
 
 template <typename R, int A0, int A1, int A2, int B0, int B1, int B2, int NT, int CC, int MINB>
@@ -269,7 +272,7 @@ __global__ void __launch_bounds__(NT, MINB) k_stage2_ct(S2ArgsCT a)
       cp_commit();
       if (tid < C * RLA) {
         const int col = tid / RLA, k = tid % RLA;
-        s_tab[tid] = two_level<V>(a.xlo, a.xhi, a.lo_bits, (m2_0 + col) * ((M1 / RLA) * k));
+        s_tab[col * (RLA + 1) + k] = two_level<V>(a.xlo, a.xhi, a.lo_bits, (m2_0 + col) * ((M1 / RLA) * k));
       }
       cp_wait_all();
       __syncthreads();

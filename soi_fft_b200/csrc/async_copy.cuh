@@ -4,6 +4,8 @@
 // kBulkWaitLimit polls; the callers set their error flag when it runs out.
 #pragma once
 
+#include <cuda.h>   // CUtensorMap
+
 namespace soi {
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -32,6 +34,16 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned by
 // orders this thread's earlier generic shared accesses before its later
 // async-proxy (bulk copy) writes to shared memory
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// global -> shared, one box of a 2-D tiled tensor map at element coordinates
+// (x, y) (x * element size a multiple of 16 bytes; the shared destination
+// aligned to the map's swizzle span), completing on `bar`.  No multicast.
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, unsigned long long *bar)
+{
+  asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+               ::"r"(smem_u32(dst)), "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+               : "memory");
+}
 
 constexpr long long kBulkWaitLimit = 1ll << 22;
 

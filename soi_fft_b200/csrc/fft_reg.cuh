@@ -220,4 +220,75 @@ __device__ __forceinline__ void tile_fft_ct(V *sm, const V *__restrict__ tw, con
   }
 }
 
+// The same tile FFT on a dense tile of C-element rows (32 bytes each) as a
+// tensor copy lays it out without swizzling: element (m, col) at m*C + col.
+// Rows visited: first stage i + r*span0, middle stage blk*span0 + i + r*RL,
+// last stage blk*RL + r, as in tile_fft_ct.  A half-warp of the first and
+// middle stages reads 4 consecutive rows x C columns (conflict-free); one of
+// the last stage reads 4 butterflies 16 rows apart, a 4-way bank conflict.
+template <typename V, int C>
+__device__ __forceinline__ V *dense_at(V *base, int m, int col)
+{
+  return base + m * C + col;
+}
+
+template <typename V, int R0, int R1, int R2, int C, int NT, class Emit>
+__device__ __forceinline__ void tile_fft_ct_dense(V *sm, const V *__restrict__ tw, const Emit &emit)
+{
+  static_assert(C * sizeof(V) == 32, "rows of 32 bytes");
+  constexpr int RL = (R2 > 1) ? R2 : R1;
+  constexpr int L = R0 * R1 * R2;
+  constexpr int span0 = L / R0;
+  {
+    constexpr int n = C * span0;
+#pragma unroll 1
+    for (int q = threadIdx.x; q < n; q += NT) {
+      const int col = q % C, i = q / C;
+      V v[R0];
+#pragma unroll
+      for (int r = 0; r < R0; ++r) v[r] = *dense_at<V, C>(sm, i + r * span0, col);
+      RegDFT<V, R0>::run(v);
+      *dense_at<V, C>(sm, i, col) = v[0];
+#pragma unroll
+      for (int k = 1; k < R0; ++k) *dense_at<V, C>(sm, i + k * span0, col) = cmul(v[k], __ldg(tw + (k - 1) * span0 + i));
+    }
+  }
+  __syncthreads();
+  if constexpr (R2 > 1) {
+    constexpr int span1 = span0 / R1;                       // = RL
+    constexpr int n = C * (L / R1);
+#pragma unroll 1
+    for (int q = threadIdx.x; q < n; q += NT) {
+      const int col = q % C, t = q / C;
+      const int blk = t / span1, i = t - blk * span1;
+      const int m0 = blk * span0 + i;
+      V v[R1];
+#pragma unroll
+      for (int r = 0; r < R1; ++r) v[r] = *dense_at<V, C>(sm, m0 + r * RL, col);
+      RegDFT<V, R1>::run(v);
+      *dense_at<V, C>(sm, m0, col) = v[0];
+#pragma unroll
+      for (int k = 1; k < R1; ++k)
+        *dense_at<V, C>(sm, m0 + k * RL, col) = cmul(v[k], __ldg(tw + (R0 - 1) * span0 + (k - 1) * span1 + i));
+    }
+    __syncthreads();
+  }
+  {
+    constexpr int n = C * (L / RL);
+#pragma unroll 1
+    for (int q = threadIdx.x; q < n; q += NT) {
+      const int col = q % C, blk = q / C;
+      int fbase;
+      if constexpr (R2 > 1) fbase = (blk / R1) + R0 * (blk % R1);
+      else fbase = blk;
+      const auto pre = emit.prepare(col, fbase);
+      V v[RL];
+#pragma unroll
+      for (int r = 0; r < RL; ++r) v[r] = *dense_at<V, C>(sm, blk * RL + r, col);
+      RegDFT<V, RL>::run(v);
+      emit.template run<RL>(col, fbase, L / RL, v, pre, blk);
+    }
+  }
+}
+
 }  // namespace soi

@@ -1,6 +1,8 @@
 // soi_b200.cu -- host side of libsoi_b200.so: the C ABI of include/soi_b200.h,
 // descriptor/plan lifecycle (pfft.c:84-267), long-double table generation
 // and the launches of the stage-1/stage-2 kernels (soi_kernels.cuh).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <math.h>
@@ -55,6 +57,9 @@ struct Plan {
   int fast2 = 0;               // 0: two-kernel stage 2, 3: persistent kernel (4: chosen, not set up)
   int f2_variant = 0;
   int f2_nt = 256;             // threads of the persistent stage-2 instance
+  int f2_boxr = 0;             // rows per pass-1 tensor copy
+  bool tma1 = false;           // tmap1 describes d_T: pass-1 tiles come by tensor copy
+  CUtensorMap tmap1;           // d_T as (2*M2 values) x (S*M1 rows), 32-byte boxes, no swizzle
   int f2_grid = 0;
   size_t f2_smem = 0;
   int discard = 1;             // drop consumed intermediate lines from L2
@@ -63,7 +68,7 @@ struct Plan {
   void *d_ctw1 = nullptr, *d_ctw2 = nullptr;   // tile-FFT twiddles of the two passes, warp read order
   double2 *d_dlo = nullptr, *d_dhi = nullptr;
   int dlo_bits = 11;
-  void (*f2ct_kernel)(S2ArgsCT) = nullptr;
+  void (*f2ct_kernel)(S2ArgsCT, const CUtensorMap) = nullptr;
   void *d_ph2 = nullptr;            // [M2] complex exp(-i pi kappa M1 k2 / M), pass-2 store order
   unsigned int *d_sync = nullptr;   // [0] err, [1] counter, [2..2+S) done1
   // staged stage 1
@@ -93,6 +98,7 @@ struct Exec {
   unsigned int *sync;          // [0] error flag (sticky), [1] task counter, [2 .. 2 + S) pass-1 counts
   int lo, hi;                  // segments computed
   cudaStream_t st;
+  const CUtensorMap *tmap = nullptr;   // T for the pass-1 tensor copies (null: cp.async staging)
 };
 
 #define CK(x)                                                                    \
@@ -312,13 +318,14 @@ int upload_regtw()
 
 // ---- stage 2 with compile-time geometry ----------------------------------------
 
-using S2KernelCT = void (*)(S2ArgsCT);
-struct S2ChoiceCT { int M1, M2, elem, nt, C; int ra[3], rb[3]; size_t smem; S2KernelCT k; };
+using S2KernelCT = void (*)(S2ArgsCT, const CUtensorMap);
+struct S2ChoiceCT { int M1, M2, elem, nt, C; int ra[3], rb[3]; int boxr; size_t smem; S2KernelCT k; };
 
 // one instance: pass-1 radices (a0, a1, a2), pass-2 radices (b0, b1, b2),
 // NT threads, C columns per task, at least MINB CTAs per SM (register bound)
 #define SOI_S2CTV(R, a0, a1, a2, b0, b1, b2, NT, C, MINB)                                         \
   { a0 * a1 * a2, b0 * b1 * b2, (int)sizeof(typename cplx_of<R>::type), NT, C, { a0, a1, a2 }, { b0, b1, b2 }, \
+    S2Geom<R, a0, a1, a2, b0, b1, b2, NT, C>::BOXR,                                             \
     (size_t)S2Geom<R, a0, a1, a2, b0, b1, b2, NT, C>::BUF * S2Geom<R, a0, a1, a2, b0, b1, b2, NT, C>::E, \
     k_stage2_ct<R, a0, a1, a2, b0, b1, b2, NT, C, MINB> }
 // the default instance: 256 threads, a whole 32-byte sector per row run, two CTAs per SM
@@ -462,6 +469,7 @@ int setup_s2ct(Plan &p, int idx)
   p.M1 = c.M1; p.M2 = c.M2;
   p.C1 = p.C2 = c.C;
   p.f2_nt = c.nt;
+  p.f2_boxr = c.boxr;
   p.f2_smem = c.smem;
   p.f2ct_kernel = c.k;
   CK(cudaFuncSetAttribute(c.k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.f2_smem));
@@ -493,7 +501,10 @@ int launch_s2ct(Plan &p, const Exec &ex)
   a.err = (int *)ex.sync; a.counter = ex.sync + 1; a.done1 = ex.sync + 2;
   // counters restart; the error flag stays set until the owner clears it
   CK(cudaMemsetAsync(ex.sync + 1, 0, (size_t)(a.S + 1) * sizeof(unsigned int), ex.st));
-  p.f2ct_kernel<<<p.f2_grid, p.f2_nt, p.f2_smem, ex.st>>>(a);
+  a.tma = ex.tmap ? 1 : 0;
+  CUtensorMap none;
+  memset(&none, 0, sizeof none);
+  p.f2ct_kernel<<<p.f2_grid, p.f2_nt, p.f2_smem, ex.st>>>(a, ex.tmap ? *ex.tmap : none);
   CK(cudaGetLastError());
   return SOI_OK;
 }
@@ -832,6 +843,50 @@ int plan_geometry(const soi_desc_t *d, size_t k, Plan &p)
 // A device plan for k segments of d's transform.  with_stream: the plan gets
 // the descriptor's stream (or its own) and timing events, as a descriptor's
 // plan; the batch driver's plans run on the batch's streams instead.
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library links no driver import library); null when the driver lacks it
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  }();
+  return fn;
+}
+
+// The pass-1 tensor map of a persistent stage-2 plan over its own T: rows of
+// 2*M2 values (M2 complex, M2*elem bytes apart), S*M1 rows (every segment),
+// boxes of one 32-byte run (C complex) x f2_boxr rows, no swizzle: a box lands
+// as f2_boxr packed 32-byte rows.  (With a swizzle mode each 32-byte row is
+// laid out over the whole swizzle span, which the dense tile has no room
+// for.)  The encoder checks base, strides and box against the hardware's
+// rules; if it refuses, the kernel stages pass-1 tiles with cp.async.
+void make_pass1_map(Plan &p)
+{
+  p.tma1 = false;
+  // measured: tensor copies win for long pass-1 tiles (M1 = 2560: 6.40 vs
+  // 6.46 ms at N = 2^29) and lose for shorter ones (M1 = 1280: 1.01 vs 0.97
+  // ms at 2^26), where the dense tile's 4-way last-stage bank conflicts cost
+  // more than the copies save; SOI_STAGE2_TMA=1 / 0 forces either
+  const int want = env_int("SOI_STAGE2_TMA", -1);
+  if (p.fast2 != 3 || !p.d_T || p.f2_boxr <= 0 || want == 0 || (want < 0 && p.M1 < 2048)) return;
+  const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return;
+  const bool f64 = p.prec == SOI_PRECISION_FP64;
+  const cuuint64_t dims[2] = { (cuuint64_t)2 * p.M2, (cuuint64_t)p.S * p.M1 };
+  const cuuint64_t strides[1] = { (cuuint64_t)p.M2 * p.elem };
+  const cuuint32_t box[2] = { (cuuint32_t)(32 / (f64 ? 8 : 4)), (cuuint32_t)p.f2_boxr };
+  const cuuint32_t estr[2] = { 1, 1 };
+  const CUresult r = enc(&p.tmap1, f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, p.d_T,
+                         dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  p.tma1 = r == CUDA_SUCCESS;
+}
+
 int make_plan(const soi_desc_t *d, size_t k, int knob_s1_nt, int knob_s2, bool with_stream, Plan **out)
 {
   Plan *p = new Plan();
@@ -859,6 +914,7 @@ int make_plan(const soi_desc_t *d, size_t k, int knob_s1_nt, int knob_s2, bool w
     return SOI_OK;
   }
   if (cudaMalloc(&p->d_T, p->S * p->Mh * p->elem) != cudaSuccess) { free_plan(p); return SOI_ERR_CUDA; }
+  make_pass1_map(*p);
   if (d->stream) {
     p->stream = (cudaStream_t)d->stream;
   } else {
@@ -916,7 +972,7 @@ int compute_impl(soi_desc_t *d, const void *in, void *out, bool stage1_only, int
     dst = p->d_io;
   }
   int rc;
-  const Exec ex{ src, p->d_T, dst, p->d_sync, seg_lo, seg_hi, st };
+  const Exec ex{ src, p->d_T, dst, p->d_sync, seg_lo, seg_hi, st, p->tma1 ? &p->tmap1 : nullptr };
   CK(cudaMemsetAsync(p->d_sync, 0, sizeof(unsigned int), st));   // error flag
   if (p->timing) CK(cudaEventRecord(p->ev[0], st));
   if ((rc = run_stage1(*p, ex))) return rc;
@@ -1364,7 +1420,7 @@ int compute_stream_impl(soi_desc_t *d, const void *const *ins, void *const *outs
     CK(cudaMemcpyAsync(buf[b], ins[i], bytes, cudaMemcpyHostToDevice, p->st_in));
     CK(cudaEventRecord(in_done[b], p->st_in));
     CK(cudaStreamWaitEvent(st, in_done[b], 0));
-    const Exec ex{ buf[b], p->d_T, buf[b], p->d_sync, 0, (int)p->S, st };
+    const Exec ex{ buf[b], p->d_T, buf[b], p->d_sync, 0, (int)p->S, st, p->tma1 ? &p->tmap1 : nullptr };
     int rc;
     if ((rc = run_stage1(*p, ex))) return rc;
     if (d->use_vlc && (rc = run_vlc(*p, ex))) return rc;
@@ -1422,7 +1478,7 @@ int compute_inverse_impl(soi_desc_t *d, const void *in, void *out)
   int rc;
   if ((rc = conj_scale(*p, in, buf, p->N, 1.0, st))) return rc;
   CK(cudaMemsetAsync(p->d_sync, 0, sizeof(unsigned int), st));
-  const Exec ex{ buf, p->d_T, buf, p->d_sync, 0, (int)p->S, st };
+  const Exec ex{ buf, p->d_T, buf, p->d_sync, 0, (int)p->S, st, p->tma1 ? &p->tmap1 : nullptr };
   if ((rc = run_stage1(*p, ex))) return rc;
   if (d->use_vlc && (rc = run_vlc(*p, ex))) return rc;
   if ((rc = run_stage2(*p, ex))) return rc;

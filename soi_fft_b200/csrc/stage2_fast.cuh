@@ -47,6 +47,7 @@
 // segments-of-interest transform).
 #pragma once
 
+#include "async_copy.cuh"
 #include "fft_reg.cuh"
 
 namespace soi {
@@ -95,6 +96,7 @@ struct S2ArgsCT {
   int S;                      // segments in this launch
   int seg_lo;                 // first segment of this launch
   int discard;
+  int tma;                    // 1: pass-1 tiles come by tensor copy (the map in the launch's second argument)
   int wait_extra;             // 0; a test sets 1 to make every pass-2 wait run out
   unsigned int *counter, *done1;
   int *err;
@@ -194,8 +196,18 @@ struct S2Geom {
   // or 8 sixteen-byte slots): pitch = (slots / C) mod slots
   static constexpr int SLOTS = 128 / E;
   static constexpr int PS2 = round_up_to_residue<M2 + M2 / RLB, SLOTS, (SLOTS / C) % SLOTS>();
-  static constexpr int BUF1 = (M1 + M1 / RLA) * C, BUF2 = PS2 * C;
-  static constexpr int BUF = BUF1 > BUF2 ? BUF1 : BUF2;
+  // pass-1 tensor copies: boxes of BOXR rows (the largest divisor of M1 of at
+  // most 256 rows that is a multiple of 32 rows, so every box starts 1024-byte
+  // aligned), into a dense tile aligned to 1024 bytes inside the buffer
+  // (slack reserved)
+  static constexpr int BOXR = [] {
+    int b = 0;
+    for (int d = 32; d <= 256; d += 32)
+      if (M1 % d == 0) b = d;
+    return b;
+  }();
+  static constexpr int BUF1 = (M1 + M1 / RLA) * C, BUF2 = PS2 * C, BUFT = M1 * C + 1024 / E;
+  static constexpr int BUF = (BUF1 > BUF2 ? BUF1 : BUF2) > BUFT ? (BUF1 > BUF2 ? BUF1 : BUF2) : BUFT;
   // shared table entries: the pass-1 step table, one row of RLA + 1 per
   // column (the pad puts a warp's C columns on different banks; at a pitch of
   // RLA every read of the table was a C-way bank conflict)
@@ -203,7 +215,7 @@ struct S2Geom {
 };
 
 template <typename R, int A0, int A1, int A2, int B0, int B1, int B2, int NT, int CC, int MINB>
-__global__ void __launch_bounds__(NT, MINB) k_stage2_ct(S2ArgsCT a)
+__global__ void __launch_bounds__(NT, MINB) k_stage2_ct(S2ArgsCT a, const __grid_constant__ CUtensorMap tmap)
 {
   using G = S2Geom<R, A0, A1, A2, B0, B1, B2, NT, CC>;
   using V = typename G::V;
@@ -211,6 +223,7 @@ __global__ void __launch_bounds__(NT, MINB) k_stage2_ct(S2ArgsCT a)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   V *buf = reinterpret_cast<V *>(smem_raw);
   __shared__ V s_tab[G::TAB];
+  __shared__ __align__(8) unsigned long long s_bar;   // pass-1 tensor copies complete here
   __shared__ unsigned int s_task[2];
   __shared__ int s_ok[2];
   const int tid = threadIdx.x;
@@ -248,10 +261,15 @@ __global__ void __launch_bounds__(NT, MINB) k_stage2_ct(S2ArgsCT a)
     s_ok[slot] = ok;
   };
   if (tid == 0) {
+    mbar_init(&s_bar, 1);
+    mbar_init_fence();
     next = atomicAdd(a.counter, 1u);
     take(0);
   }
   __syncthreads();
+  // the dense pass-1 tile of the tensor-copy path (rows of C elements), 1024-byte aligned
+  V *tile1 = reinterpret_cast<V *>(smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u));
+  unsigned int bphase = 0;                                  // parity of s_bar's current phase
 
   for (int iter = 0;; ++iter) {
     const int slot = iter & 1;
@@ -262,22 +280,50 @@ __global__ void __launch_bounds__(NT, MINB) k_stage2_ct(S2ArgsCT a)
     V *Tseg = reinterpret_cast<V *>(a.T) + (size_t)(a.seg_lo + seg) * ((size_t)M1 * M2);
     if (kind == 1) {
       const int m2_0 = tile * C;
-      // rows m1 of C columns: CPR1 chunks of 16 bytes each
-      constexpr int EPC = 16 / G::E;                        // elements per 16-byte chunk
-      constexpr int CPR1 = G::CPR1;
-      for (int q = tid; q < M1 * CPR1; q += NT) {
-        const int row = q / CPR1, h = q % CPR1;
-        cp_async_16cg(buf + (row + row / RLA) * C + h * EPC, Tseg + row * M2 + m2_0 + h * EPC);
-      }
-      cp_commit();
-      if (tid < C * RLA) {
-        const int col = tid / RLA, k = tid % RLA;
-        s_tab[col * (RLA + 1) + k] = two_level<V>(a.xlo, a.xhi, a.lo_bits, (m2_0 + col) * ((M1 / RLA) * k));
-      }
-      cp_wait_all();
-      __syncthreads();
       EmitColsCT<V, C, M2, RLA> e{ Tseg, m2_0, s_tab, &a };
-      tile_fft_ct<V, A0, A1, A2, C, C, 1, NT>(buf, reinterpret_cast<const V *>(a.tw1), e);
+      if (a.tma) {
+        // C columns x M1 rows (32-byte runs 16 KB apart) by M1 / BOXR tensor
+        // copies: the TMA engine gathers the rows, off the load/store path
+        if (tid == 0) {
+          static_assert(G::BOXR > 0 && M1 % G::BOXR == 0, "whole boxes");
+          fence_proxy_async_smem();                         // the previous task's reads of the tile come first
+          mbar_expect_tx(&s_bar, (unsigned int)(M1 * C * G::E));
+          const int y0 = (a.seg_lo + seg) * M1;
+#pragma unroll 1
+          for (int b = 0; b < M1 / G::BOXR; ++b)
+            tma_load_2d(tile1 + b * G::BOXR * C, &tmap, 2 * m2_0, y0 + b * G::BOXR, &s_bar);
+        }
+        if (tid < C * RLA) {
+          const int col = tid / RLA, k = tid % RLA;
+          s_tab[col * (RLA + 1) + k] = two_level<V>(a.xlo, a.xhi, a.lo_bits, (m2_0 + col) * ((M1 / RLA) * k));
+        }
+        long long it = 0;
+        while (!mbar_try_wait(&s_bar, bphase)) {
+          if (++it > kBulkWaitLimit) {
+            if (tid == 0) atomicExch(a.err, 1);             // no further tasks are taken
+            break;
+          }
+        }
+        bphase ^= 1u;
+        __syncthreads();
+        tile_fft_ct_dense<V, A0, A1, A2, C, NT>(tile1, reinterpret_cast<const V *>(a.tw1), e);
+      } else {
+        // rows m1 of C columns: CPR1 chunks of 16 bytes each
+        constexpr int EPC = 16 / G::E;                        // elements per 16-byte chunk
+        constexpr int CPR1 = G::CPR1;
+        for (int q = tid; q < M1 * CPR1; q += NT) {
+          const int row = q / CPR1, h = q % CPR1;
+          cp_async_16cg(buf + (row + row / RLA) * C + h * EPC, Tseg + row * M2 + m2_0 + h * EPC);
+        }
+        cp_commit();
+        if (tid < C * RLA) {
+          const int col = tid / RLA, k = tid % RLA;
+          s_tab[col * (RLA + 1) + k] = two_level<V>(a.xlo, a.xhi, a.lo_bits, (m2_0 + col) * ((M1 / RLA) * k));
+        }
+        cp_wait_all();
+        __syncthreads();
+        tile_fft_ct<V, A0, A1, A2, C, C, 1, NT>(buf, reinterpret_cast<const V *>(a.tw1), e);
+      }
       __syncthreads();                                        // every store of the tile is issued
       if (tid == 0) {
         __threadfence();

@@ -238,3 +238,27 @@ def test_bulk_copy_staging_equals_cp_async_staging(N, S, prec, monkeypatch):
         finally:
             d.free()
     assert torch.equal(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("N,S,prec", [(1 << 20, 16, sb.PRECISION_SPLIT_FP32), (1 << 22, 32, sb.PRECISION_SPLIT_FP32),
+                                      (1 << 26, 128, sb.PRECISION_SPLIT_FP32), (1 << 20, 8, sb.PRECISION_FP64),
+                                      (1 << 24, 64, sb.PRECISION_FP64)])
+@pytest.mark.parametrize("band", ["all", (3, 7)])
+def test_tensor_copy_staging_equals_cp_async_staging(N, S, prec, band, monkeypatch):
+    # the persistent stage 2 stages pass-1 tiles by tensor copies (a swizzled
+    # dense tile) or by cp.async (a padded tile): the same arithmetic on the
+    # same values, so the outputs are identical
+    x = _input(N, prec)
+    lo, hi = (0, S) if band == "all" else band
+    outs = []
+    for tma in ("1", "0"):
+        monkeypatch.setenv("SOI_STAGE2_TMA", tma)
+        d = _desc(N, S, prec)
+        try:
+            y = torch.zeros_like(x)
+            d.compute_segments(x, y, lo, hi)
+            torch.cuda.synchronize()
+            outs.append(y)
+        finally:
+            d.free()
+    assert torch.equal(outs[0], outs[1])

@@ -58,6 +58,7 @@ struct Plan {
   int f2_variant = 0;
   int f2_nt = 256;             // threads of the persistent stage-2 instance
   int f2_boxr = 0;             // rows per pass-1 tensor copy
+  int f2_lead = 0;             // stage-2 schedule: pass-1 tasks of a block ahead of the interleave
   bool tma1 = false;           // tmap1 describes d_T: pass-1 tiles come by tensor copy
   CUtensorMap tmap1;           // d_T as (2*M2 values) x (S*M1 rows), 32-byte boxes, no swizzle
   int f2_grid = 0;
@@ -478,6 +479,19 @@ int setup_s2ct(Plan &p, int idx)
   CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, p.device));
   if (occ < 1) return SOI_ERR_UNSUPPORTED;
   p.f2_grid = occ * nsm;
+  {
+    // schedule lead: a pass-2 task of segment b must not be claimed before
+    // the last pass-1 task of b has had time to finish, i.e. about one task
+    // per resident CTA later; a lead of that many pass-1 tasks keeps the
+    // waits away and the rest of the block interleaved (measured in the split
+    // form at N = 2^29: 6.31 ms with a lead of 256-384 of 512, 6.44 with 512,
+    // 6.87 with 0).  FP64 keeps every pass-1 task ahead (lead = NT1): at
+    // N = 2^28 the interleave measured 8.54 ms against 8.22-8.29.
+    const int nt1 = c.M2 / c.C;
+    const int dflt = p.prec == SOI_PRECISION_FP64 ? nt1 : std::min(nt1, p.f2_grid);
+    const int lead = env_int("SOI_STAGE2_LEAD", dflt);
+    p.f2_lead = lead < 0 ? 0 : lead > nt1 ? nt1 : lead;
+  }
   int rc = p.prec == SOI_PRECISION_FP64 ? build_ct_tables<double>(p, c) : build_ct_tables<float>(p, c);
   if (rc) return rc;
   p.discard = env_int("SOI_STAGE2_DISCARD", 1);
@@ -498,6 +512,7 @@ int launch_s2ct(Plan &p, const Exec &ex)
   a.S = ex.hi - ex.lo; a.seg_lo = ex.lo;
   a.discard = p.discard;
   a.wait_extra = p.wait_extra;
+  a.lead = p.f2_lead;
   a.err = (int *)ex.sync; a.counter = ex.sync + 1; a.done1 = ex.sync + 2;
   // counters restart; the error flag stays set until the owner clears it
   CK(cudaMemsetAsync(ex.sync + 1, 0, (size_t)(a.S + 1) * sizeof(unsigned int), ex.st));

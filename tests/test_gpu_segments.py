@@ -262,3 +262,27 @@ def test_tensor_copy_staging_equals_cp_async_staging(N, S, prec, band, monkeypat
         finally:
             d.free()
     assert torch.equal(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("N,S,prec", [(1 << 22, 32, sb.PRECISION_SPLIT_FP32), (1 << 20, 8, sb.PRECISION_FP64)])
+@pytest.mark.parametrize("band", ["all", (2, 5)])
+def test_stage2_schedule_does_not_change_results(N, S, prec, band, monkeypatch):
+    # the persistent stage 2's task order (how far pass 1 of the next segment
+    # runs ahead of pass 2 of the current one) only moves work in time
+    x = _input(N, prec)
+    lo, hi = (0, S) if band == "all" else band
+    outs = []
+    for lead in ("0", "7", None):
+        if lead is None:
+            monkeypatch.delenv("SOI_STAGE2_LEAD", raising=False)
+        else:
+            monkeypatch.setenv("SOI_STAGE2_LEAD", lead)
+        d = _desc(N, S, prec)
+        try:
+            y = torch.zeros_like(x)
+            d.compute_segments(x, y, lo, hi)
+            torch.cuda.synchronize()
+            outs.append(y)
+        finally:
+            d.free()
+    assert torch.equal(outs[0], outs[2]) and torch.equal(outs[1], outs[2])

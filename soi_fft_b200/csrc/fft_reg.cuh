@@ -224,8 +224,9 @@ __device__ __forceinline__ void tile_fft_ct(V *sm, const V *__restrict__ tw, con
 // tensor copy lays it out without swizzling: element (m, col) at m*C + col.
 // Rows visited: first stage i + r*span0, middle stage blk*span0 + i + r*RL,
 // last stage blk*RL + r, as in tile_fft_ct.  A half-warp of the first and
-// middle stages reads 4 consecutive rows x C columns (conflict-free); one of
-// the last stage reads 4 butterflies 16 rows apart, a 4-way bank conflict.
+// middle stages reads 4 consecutive rows x C columns (conflict-free); the last
+// stage's half-warp (4 butterflies 16 rows apart) reads in a per-butterfly
+// row order that keeps it conflict-free too.
 template <typename V, int C>
 __device__ __forceinline__ V *dense_at(V *base, int m, int col)
 {
@@ -282,11 +283,19 @@ __device__ __forceinline__ void tile_fft_ct_dense(V *sm, const V *__restrict__ t
       if constexpr (R2 > 1) fbase = (blk / R1) + R0 * (blk % R1);
       else fbase = blk;
       const auto pre = emit.prepare(col, fbase);
-      V v[RL];
+      // a half-warp holds 4 butterflies 16 rows apart, whose rows share banks:
+      // each reads its rows in the order r ^ (blk & 3), which puts the four
+      // on different banks, and two conditional swaps restore the order
+      const int x = blk & 3;
+      V u[RL], v[RL];
 #pragma unroll
-      for (int r = 0; r < RL; ++r) v[r] = *dense_at<V, C>(sm, blk * RL + r, col);
-      RegDFT<V, RL>::run(v);
-      emit.template run<RL>(col, fbase, L / RL, v, pre, blk);
+      for (int r = 0; r < RL; ++r) u[r] = *dense_at<V, C>(sm, blk * RL + (r ^ x), col);
+#pragma unroll
+      for (int r = 0; r < RL; ++r) v[r] = (x & 1) ? u[r ^ 1] : u[r];
+#pragma unroll
+      for (int r = 0; r < RL; ++r) u[r] = (x & 2) ? v[r ^ 2] : v[r];
+      RegDFT<V, RL>::run(u);
+      emit.template run<RL>(col, fbase, L / RL, u, pre, blk);
     }
   }
 }

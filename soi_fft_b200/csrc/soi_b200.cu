@@ -883,12 +883,10 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 void make_pass1_map(Plan &p)
 {
   p.tma1 = false;
-  // measured: tensor copies win for long pass-1 tiles (M1 = 2560: 6.40 vs
-  // 6.46 ms at N = 2^29) and lose for shorter ones (M1 = 1280: 1.01 vs 0.97
-  // ms at 2^26), where the dense tile's 4-way last-stage bank conflicts cost
-  // more than the copies save; SOI_STAGE2_TMA=1 / 0 forces either
-  const int want = env_int("SOI_STAGE2_TMA", -1);
-  if (p.fast2 != 3 || !p.d_T || p.f2_boxr <= 0 || want == 0 || (want < 0 && p.M1 < 2048)) return;
+  // measured against cp.async staging: 6.09 vs 6.36 ms at N = 2^29 (split),
+  // 0.99 vs 1.00 ms at 2^26, 8.09 vs 8.33 ms at 2^28 in FP64;
+  // SOI_STAGE2_TMA=0 selects cp.async (tests compare the two)
+  if (p.fast2 != 3 || !p.d_T || p.f2_boxr <= 0 || !env_int("SOI_STAGE2_TMA", 1)) return;
   const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
   if (!enc) return;
   const bool f64 = p.prec == SOI_PRECISION_FP64;

@@ -19,6 +19,14 @@ template <> struct cplx_of<double> { using type = double2; };
 template <typename V> __device__ __forceinline__ V cmk(decltype(V::x) a, decltype(V::x) b) { V r; r.x = a; r.y = b; return r; }
 template <typename V> __device__ __forceinline__ V cadd(V a, V b) { return cmk<V>(a.x + b.x, a.y + b.y); }
 template <typename V> __device__ __forceinline__ V csub(V a, V b) { return cmk<V>(a.x - b.x, a.y - b.y); }
+// FP32: one packed add (FADD2) per complex add or subtract, the same IEEE
+// roundings as two scalar adds in half the instructions (the butterflies are
+// mostly adds; measured 1.2 % on stage 1 and 1.7 % on stage 2 at N = 2^29)
+template <> __device__ __forceinline__ float2 cadd<float2>(float2 a, float2 b) { return __fadd2_rn(a, b); }
+template <> __device__ __forceinline__ float2 csub<float2>(float2 a, float2 b)
+{
+  return __fadd2_rn(a, make_float2(-b.x, -b.y));
+}
 template <typename V> __device__ __forceinline__ V cmul(V a, V b)
 {
   return cmk<V>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);

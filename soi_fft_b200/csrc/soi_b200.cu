@@ -58,7 +58,7 @@ struct Plan {
   int f2_variant = 0;
   int f2_nt = 256;             // threads of the persistent stage-2 instance
   int f2_boxr = 0;             // rows per pass-1 tensor copy
-  int f2_lead = 0;             // stage-2 schedule: pass-1 tasks of a block ahead of the interleave
+  int f2_tail = 0;             // stage-2 schedule: pass-2 tasks that end a block
   bool tma1 = false;           // tmap1 describes d_T: pass-1 tiles come by tensor copy
   CUtensorMap tmap1;           // d_T as (2*M2 values) x (S*M1 rows), 32-byte boxes, no swizzle
   int f2_grid = 0;
@@ -480,17 +480,21 @@ int setup_s2ct(Plan &p, int idx)
   if (occ < 1) return SOI_ERR_UNSUPPORTED;
   p.f2_grid = occ * nsm;
   {
-    // schedule lead: a pass-2 task of segment b must not be claimed before
-    // the last pass-1 task of b has had time to finish, i.e. about one task
-    // per resident CTA later; a lead of that many pass-1 tasks keeps the
-    // waits away and the rest of the block interleaved (measured in the split
-    // form at N = 2^29: 6.31 ms with a lead of 256-384 of 512, 6.44 with 512,
-    // 6.87 with 0).  FP64 keeps every pass-1 task ahead (lead = NT1): at
-    // N = 2^28 the interleave measured 8.54 ms against 8.22-8.29.
-    const int nt1 = c.M2 / c.C;
-    const int dflt = p.prec == SOI_PRECISION_FP64 ? nt1 : std::min(nt1, p.f2_grid);
-    const int lead = env_int("SOI_STAGE2_LEAD", dflt);
-    p.f2_lead = lead < 0 ? 0 : lead > nt1 ? nt1 : lead;
+    // schedule tail: a segment's pass-2 tasks must not be claimed before its
+    // last pass-1 task has had time to finish, about one task per resident
+    // CTA later; ending each block with that many pass-2 tasks keeps most
+    // waits away while the rest of the block interleaves the two passes.
+    // Measured in the split form: N = 2^29 (NT2 = 640) 5.90 ms with a tail of
+    // 296 (the grid), 6.18 with 640, 6.00 with 150; N = 2^26 (NT2 = 320) 0.98
+    // ms with 320, 1.11 with 296.  With every CTA holding one claimed task
+    // ahead of the running one, a block needs about two tasks per CTA of
+    // pass 2 for the interleave to pay; smaller blocks, and FP64 (8.54 ms
+    // interleaved against 8.22-8.29 at N = 2^28), keep every pass-1 task of a
+    // block ahead of its pass-2 tasks (tail = NT2).
+    const int nt2 = c.M1 / c.C;
+    const int dflt = (p.prec == SOI_PRECISION_FP64 || nt2 < 2 * p.f2_grid) ? nt2 : p.f2_grid;
+    const int tail = env_int("SOI_STAGE2_TAIL", dflt);
+    p.f2_tail = tail < 0 ? 0 : tail > nt2 ? nt2 : tail;
   }
   int rc = p.prec == SOI_PRECISION_FP64 ? build_ct_tables<double>(p, c) : build_ct_tables<float>(p, c);
   if (rc) return rc;
@@ -512,7 +516,7 @@ int launch_s2ct(Plan &p, const Exec &ex)
   a.S = ex.hi - ex.lo; a.seg_lo = ex.lo;
   a.discard = p.discard;
   a.wait_extra = p.wait_extra;
-  a.lead = p.f2_lead;
+  a.tail = p.f2_tail;
   a.err = (int *)ex.sync; a.counter = ex.sync + 1; a.done1 = ex.sync + 2;
   // counters restart; the error flag stays set until the owner clears it
   CK(cudaMemsetAsync(ex.sync + 1, 0, (size_t)(a.S + 1) * sizeof(unsigned int), ex.st));

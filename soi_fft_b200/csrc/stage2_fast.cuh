@@ -98,7 +98,7 @@ struct S2ArgsCT {
   int discard;
   int tma;                    // 1: pass-1 tiles come by tensor copy (the map in the launch's second argument)
   int wait_extra;             // 0; a test sets 1 to make every pass-2 wait run out
-  int lead;                   // pass-1 tasks of a block ahead of its interleaved part (0 .. M2/C)
+  int tail;                   // pass-2 tasks that end a block after its interleaved part (0 .. M1/C)
   unsigned int *counter, *done1;
   int *err;
 };
@@ -229,23 +229,25 @@ __global__ void __launch_bounds__(NT, MINB) k_stage2_ct(S2ArgsCT a, const __grid
   __shared__ int s_ok[2];
   const int tid = threadIdx.x;
   const unsigned int total = (unsigned int)a.S * G::PER;
-  // task index -> (pass, segment, tile): P1(0), then per block b = 0 .. S-2
-  // the first `lead` pass-1 tasks of segment b+1 followed by its other pass-1
-  // tasks interleaved in proportion with the pass-2 tasks of segment b, then
-  // P2(S-1).  Segment b+1's intermediate grows while b's is consumed (and
-  // discarded), which keeps fewer bytes live in L2 than all of P1(b+1)
-  // before P2(b) (lead = NT1).
-  const int lead = a.lead;
+  // task index -> (pass, segment, tile): P1(0); then per block b = 0 .. S-2
+  // the pass-1 tasks of segment b+1 interleaved in proportion with the first
+  // NT2 - tail pass-2 tasks of segment b, followed by its last `tail` pass-2
+  // tasks; then P2(S-1).  Segment b+1's intermediate grows while b's is
+  // consumed (and discarded), so about one segment's intermediate is live in
+  // L2, and a segment's pass-2 tasks come at least `tail` claims after its
+  // last pass-1 task, by when that task has usually finished (with tail =
+  // NT2 every pass-1 task of b+1 comes before the pass-2 tasks of b).
+  const int tail = a.tail;
   auto decode = [&](unsigned int t, int &kind, int &seg, int &tile) {
     if (t < (unsigned int)G::NT1) { kind = 1; seg = 0; tile = (int)t; return; }
     const unsigned int u = t - G::NT1;
     const int blk = (int)(u / G::PER), r = (int)(u % G::PER);
     if (blk >= a.S - 1) { kind = 2; seg = blk; tile = r; return; }
-    if (r < lead) { kind = 1; seg = blk + 1; tile = r; return; }
-    const int rr = r - lead, n1 = G::NT1 - lead, nn = n1 + G::NT2;
-    const int c0 = rr * n1 / nn, c1 = (rr + 1) * n1 / nn;   // pass-1 tasks among the first rr (rr + 1)
-    if (c1 > c0) { kind = 1; seg = blk + 1; tile = lead + c0; }
-    else { kind = 2; seg = blk; tile = rr - c0; }
+    const int n2i = G::NT2 - tail, ni = G::NT1 + n2i;    // the interleaved part
+    if (r >= ni) { kind = 2; seg = blk; tile = n2i + (r - ni); return; }
+    const int c0 = r * G::NT1 / ni, c1 = (r + 1) * G::NT1 / ni;   // pass-1 tasks among the first r (r + 1)
+    if (c1 > c0) { kind = 1; seg = blk + 1; tile = c0; }
+    else { kind = 2; seg = blk; tile = r - c0; }
   };
   unsigned int next = 0;
   // thread 0: take the claimed task, claim the one after it, and for a

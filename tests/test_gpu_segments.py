@@ -267,16 +267,16 @@ def test_tensor_copy_staging_equals_cp_async_staging(N, S, prec, band, monkeypat
 @pytest.mark.parametrize("N,S,prec", [(1 << 22, 32, sb.PRECISION_SPLIT_FP32), (1 << 20, 8, sb.PRECISION_FP64)])
 @pytest.mark.parametrize("band", ["all", (2, 5)])
 def test_stage2_schedule_does_not_change_results(N, S, prec, band, monkeypatch):
-    # the persistent stage 2's task order (how far pass 1 of the next segment
-    # runs ahead of pass 2 of the current one) only moves work in time
+    # the persistent stage 2's task order (how pass 1 of the next segment is
+    # interleaved with pass 2 of the current one) only moves work in time
     x = _input(N, prec)
     lo, hi = (0, S) if band == "all" else band
     outs = []
-    for lead in ("0", "7", None):
-        if lead is None:
-            monkeypatch.delenv("SOI_STAGE2_LEAD", raising=False)
+    for tail in ("0", "7", None):
+        if tail is None:
+            monkeypatch.delenv("SOI_STAGE2_TAIL", raising=False)
         else:
-            monkeypatch.setenv("SOI_STAGE2_LEAD", lead)
+            monkeypatch.setenv("SOI_STAGE2_TAIL", tail)
         d = _desc(N, S, prec)
         try:
             y = torch.zeros_like(x)

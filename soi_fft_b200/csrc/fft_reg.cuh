@@ -210,7 +210,7 @@ __device__ __forceinline__ void tile_fft_ct(V *sm, const V *__restrict__ tw, con
       if constexpr (R2 > 1) fbase = (blk / R1) + R0 * (blk % R1);
       else fbase = blk;
       // the epilogue's own loads go out before the last radix's arithmetic
-      const auto pre = emit.prepare(col, fbase);
+      const auto pre = emit.prepare(col, fbase, blk);
       V v[RL];
 #pragma unroll
       for (int r = 0; r < RL; ++r) v[r] = p[r * PP];
@@ -282,7 +282,7 @@ __device__ __forceinline__ void tile_fft_ct_dense(V *sm, const V *__restrict__ t
       int fbase;
       if constexpr (R2 > 1) fbase = (blk / R1) + R0 * (blk % R1);
       else fbase = blk;
-      const auto pre = emit.prepare(col, fbase);
+      const auto pre = emit.prepare(col, fbase, blk);
       // a half-warp holds 4 butterflies 16 rows apart, whose rows share banks:
       // each reads its rows in the order r ^ (blk & 3), which puts the four
       // on different banks, and two conditional swaps restore the order

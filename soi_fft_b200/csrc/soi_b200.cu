@@ -67,6 +67,7 @@ struct Plan {
   int wait_extra = 0;          // failure test: pass-2 waits for a count that never comes
   void *d_amp = nullptr;            // [M1][M2] real demodulation amplitude, pass-2 store order
   void *d_ctw1 = nullptr, *d_ctw2 = nullptr;   // tile-FFT twiddles of the two passes, warp read order
+  void *d_base1 = nullptr, *d_step1 = nullptr; // pass-1 epilogue bases and steps, warp read order
   double2 *d_dlo = nullptr, *d_dhi = nullptr;
   int dlo_bits = 11;
   void (*f2ct_kernel)(S2ArgsCT, const CUtensorMap) = nullptr;
@@ -458,6 +459,27 @@ int build_ct_tables(Plan &p, const S2ChoiceCT &c)
     ph[2 * pos + 1] = (R)o[1];
   }
   if ((rc = upload(&p.d_ph2, ph.data(), ph.size() * sizeof(R)))) return rc;
+  // pass-1 epilogue: base w_{M'}^(m2*fbase(blk)) at [(t*NB + blk)*C + col]
+  // (m2 = C*t + col, NB = M1/RL butterflies of the last radix) and steps
+  // w_{M'}^(m2*(M1/RL)*k) at [m2*RL + k], in long double, rounded once
+  {
+    const long long RLA = c.ra[2] > 1 ? c.ra[2] : c.ra[1], NB = M1 / RLA, Mp = M1 * M2;
+    auto root = [&](long long e, R *o) {
+      long double ang = -2.0L * kPi * (long double)(e % Mp) / (long double)Mp;
+      o[0] = (R)cosl(ang);
+      o[1] = (R)sinl(ang);
+    };
+    std::vector<R> bt(2 * (size_t)M2 * NB), st(2 * (size_t)M2 * RLA);
+    for (long long t = 0; t < M2 / C; ++t)
+      for (long long blk = 0; blk < NB; ++blk) {
+        const long long fbase = c.ra[2] > 1 ? blk / c.ra[1] + c.ra[0] * (blk % c.ra[1]) : blk;
+        for (long long col = 0; col < C; ++col) root((C * t + col) * fbase, &bt[2 * (size_t)((t * NB + blk) * C + col)]);
+      }
+    for (long long m2 = 0; m2 < M2; ++m2)
+      for (long long k = 0; k < RLA; ++k) root(m2 * NB * k, &st[2 * (size_t)(m2 * RLA + k)]);
+    if ((rc = upload(&p.d_base1, bt.data(), bt.size() * sizeof(R)))) return rc;
+    if ((rc = upload(&p.d_step1, st.data(), st.size() * sizeof(R)))) return rc;
+  }
   std::vector<R> w1 = tile_twiddles<R>(c.ra[0], c.ra[1], c.ra[2]), w2 = tile_twiddles<R>(c.rb[0], c.rb[1], c.rb[2]);
   if ((rc = upload(&p.d_ctw1, w1.data(), w1.size() * sizeof(R)))) return rc;
   if ((rc = upload(&p.d_ctw2, w2.data(), w2.size() * sizeof(R)))) return rc;
@@ -510,9 +532,9 @@ int setup_s2ct(Plan &p, int idx)
 int launch_s2ct(Plan &p, const Exec &ex)
 {
   S2ArgsCT a;
-  a.T = ex.T; a.out = ex.out; a.tw1 = p.d_ctw1; a.tw2 = p.d_ctw2; a.xlo = p.d_xlo; a.xhi = p.d_xhi;
+  a.T = ex.T; a.out = ex.out; a.tw1 = p.d_ctw1; a.tw2 = p.d_ctw2; a.base1 = p.d_base1; a.step1 = p.d_step1;
   a.amp = p.d_amp; a.dlo = p.d_dlo; a.dhi = p.d_dhi; a.ph2 = p.d_ph2;
-  a.lo_bits = p.lo_bits; a.dlo_bits = p.dlo_bits; a.M = (int)p.M;
+  a.dlo_bits = p.dlo_bits; a.M = (int)p.M;
   a.S = ex.hi - ex.lo; a.seg_lo = ex.lo;
   a.discard = p.discard;
   a.wait_extra = p.wait_extra;
@@ -808,7 +830,7 @@ void free_plan(Plan *p)
   cudaSetDevice(p->device);
   void *bufs[] = { p->d_filt, p->d_phase, p->d_twS, p->d_tw1, p->d_tw2, p->d_winv, p->d_wsmall,
                    p->d_permS, p->d_perm1, p->d_perm2, p->d_xlo, p->d_xhi, p->d_T, p->d_io, p->d_io2,
-                   p->d_vlc_words, p->d_vlc_n, p->d_vlc_emax, p->d_sync, p->d_filt2, p->d_amp, p->d_dlo, p->d_dhi, p->d_ph2, p->d_ctw1, p->d_ctw2 };
+                   p->d_vlc_words, p->d_vlc_n, p->d_vlc_emax, p->d_sync, p->d_filt2, p->d_amp, p->d_dlo, p->d_dhi, p->d_ph2, p->d_ctw1, p->d_ctw2, p->d_base1, p->d_step1 };
   for (void *b : bufs) if (b) cudaFree(b);
   for (auto &e : p->ev) if (e) cudaEventDestroy(e);
   for (auto &e : p->sev) if (e) cudaEventDestroy(e);

@@ -16,10 +16,11 @@
 // and stores, pass-2 output stores) is one full 32-byte sector, so each L2
 // request moves a whole sector.
 //
-// Epilogue factors come from per-task tables instead of scattered lookups.
-// Pass 1: w_{M'}^(m2*f) for f = fbase + fstep*k is base(m2*fbase) times
-// step[col][k] = w_{M'}^(m2*fstep*k), the C x RL step table built per task in
-// shared memory (row pitch RL + 1).  Pass 2: W_inv[k], k = k1 + M1*k2, is
+// Epilogue factors come from tables instead of scattered lookups.  Pass 1:
+// w_{M'}^(m2*f) for f = fbase + fstep*k is base(m2*fbase) times
+// step[col][k] = w_{M'}^(m2*fstep*k); both come from tables laid out in the
+// order the warps read them, the task's C x RL steps copied into shared memory
+// (row pitch RL + 1).  Pass 2: W_inv[k], k = k1 + M1*k2, is
 // amp[min(k, M-k)] * ph(k1) * ph(M1*k2) with ph(k) = exp(-i pi kappa k/M);
 // ph(k1) per task in shared memory, amp and ph(M1*k2) from tables laid out in
 // the order the last radix stage stores its outputs, and the tile twiddles
@@ -87,11 +88,12 @@ struct S2ArgsCT {
   void *T;                    // [S][Mh] pass-1 input, intermediate in place
   void *out;                  // [S][M]
   const void *tw1, *tw2;      // tile twiddles of the two passes, warp read order
-  const double2 *xlo, *xhi;   // w_{M'}^e two-level, FP64
+  const void *base1;          // [M2/C][M1/RL][C] pass-1 epilogue bases w_{M'}^(m2*fbase), warp read order
+  const void *step1;          // [M2][RL] pass-1 epilogue steps w_{M'}^(m2*(M1/RL)*k)
   const void *amp;            // [M1][M2] real, pass-2 store order per task
   const double2 *dlo, *dhi;   // exp(-i pi kappa k/M) two-level, FP64
   const void *ph2;            // [M2] complex exp(-i pi kappa M1 k2 / M), pass-2 store order
-  int lo_bits, dlo_bits;
+  int dlo_bits;
   int M;
   int S;                      // segments in this launch
   int seg_lo;                 // first segment of this launch
@@ -112,20 +114,22 @@ __device__ __forceinline__ V two_level(const double2 *lo, const double2 *hi, int
 }
 
 template <typename V, int C1, int M2, int RL> struct EmitColsCT {
-  V *Tseg; int m2_0; const V *step; const S2ArgsCT *a;
-  // w_{M'}^(m2*fbase), loaded and formed before the last radix
-  __device__ __forceinline__ V prepare(int col, int fbase) const
+  V *Tseg; int m2_0; const V *step; const V *base; const S2ArgsCT *a;
+  // w_{M'}^(m2*fbase) of butterfly blk: base[blk*C + col], the task's slice of a
+  // table in the order the last radix stage's warps read it (one cache line per
+  // warp load), loaded before the last radix
+  __device__ __forceinline__ V prepare(int col, int, int blk) const
   {
-    return two_level<V>(a->xlo, a->xhi, a->lo_bits, (m2_0 + col) * fbase);
+    return __ldg(base + blk * C1 + col);
   }
-  template <int RLx> __device__ __forceinline__ void run(int col, int fbase, int fstep, V *v, V base, int) const
+  template <int RLx> __device__ __forceinline__ void run(int col, int fbase, int fstep, V *v, V base_f, int) const
   {
     static_assert(RLx == RL, "last radix");
     const int m2 = m2_0 + col;
     V *dst = Tseg + fbase * M2 + m2;
-    dst[0] = cmul(v[0], base);
+    dst[0] = cmul(v[0], base_f);
 #pragma unroll
-    for (int k = 1; k < RL; ++k) dst[k * fstep * M2] = cmul(v[k], cmul(base, step[col * (RL + 1) + k]));
+    for (int k = 1; k < RL; ++k) dst[k * fstep * M2] = cmul(v[k], cmul(base_f, step[col * (RL + 1) + k]));
   }
 };
 
@@ -137,7 +141,7 @@ struct NoPre {};
 // consecutive butterflies x C rows) are one cache line each
 template <typename V, int M1, int M2, int C, int RL, bool BATCH> struct EmitRowsCT {
   V *oseg; int k1_0; const V *ph1; const S2ArgsCT *a;
-  __device__ __forceinline__ NoPre prepare(int, int) const { return NoPre{}; }
+  __device__ __forceinline__ NoPre prepare(int, int, int) const { return NoPre{}; }
   template <int RLx> __device__ __forceinline__ void run(int col, int fbase, int fstep, V *v, NoPre, int blk) const
   {
     static_assert(RLx == RL, "last radix");
@@ -293,7 +297,8 @@ __global__ void __launch_bounds__(NT, MINB) k_stage2_ct(S2ArgsCT a, const __grid
     V *Tseg = reinterpret_cast<V *>(a.T) + (size_t)(a.seg_lo + seg) * ((size_t)M1 * M2);
     if (kind == 1) {
       const int m2_0 = tile * C;
-      EmitColsCT<V, C, M2, RLA> e{ Tseg, m2_0, s_tab, &a };
+      EmitColsCT<V, C, M2, RLA> e{ Tseg, m2_0, s_tab,
+                                   reinterpret_cast<const V *>(a.base1) + (size_t)tile * (M1 / RLA) * C, &a };
       if (a.tma) {
         // C columns x M1 rows (32-byte runs 16 KB apart) by M1 / BOXR tensor
         // copies: the TMA engine gathers the rows, off the load/store path
@@ -308,7 +313,7 @@ __global__ void __launch_bounds__(NT, MINB) k_stage2_ct(S2ArgsCT a, const __grid
         }
         if (tid < C * RLA) {
           const int col = tid / RLA, k = tid % RLA;
-          s_tab[col * (RLA + 1) + k] = two_level<V>(a.xlo, a.xhi, a.lo_bits, (m2_0 + col) * ((M1 / RLA) * k));
+          s_tab[col * (RLA + 1) + k] = __ldg(reinterpret_cast<const V *>(a.step1) + (m2_0 + col) * RLA + k);
         }
         long long it = 0;
         while (!mbar_try_wait(&s_bar, bphase)) {
@@ -331,7 +336,7 @@ __global__ void __launch_bounds__(NT, MINB) k_stage2_ct(S2ArgsCT a, const __grid
         cp_commit();
         if (tid < C * RLA) {
           const int col = tid / RLA, k = tid % RLA;
-          s_tab[col * (RLA + 1) + k] = two_level<V>(a.xlo, a.xhi, a.lo_bits, (m2_0 + col) * ((M1 / RLA) * k));
+          s_tab[col * (RLA + 1) + k] = __ldg(reinterpret_cast<const V *>(a.step1) + (m2_0 + col) * RLA + k);
         }
         cp_wait_all();
         __syncthreads();

@@ -61,9 +61,9 @@ CPU_SAMPLE_LOG2N = 24
 # L2 residency depends on the segment size, so a smaller M' would not carry).
 KERNELS = {
     "stage1": ("k_conv_sfft_tS (stage 1: convolution + S-point FFTs + transposed store)", 1156.7 / 1208.0,
-               "ncu at N=2^26, S=128 (profiles/k_conv_sfft_tS_N2e26_S128_split.md), scaled by the units processed"),
+               "ncu at N=2^26, S=128 (same kernel instance), scaled by the units processed"),
     "stage2": ("k_stage2_ct (stage 2: M'-point four-step FFT + demodulation + discard)", 8724.6 / 4831.8,
-               "ncu at N=2^28, S=64, same M' tiles (profiles/k_stage2_ct_N2e28_S64_split.md), scaled by the segments"),
+               "ncu at N=2^28, S=64 (same M' tiles), scaled by the segments"),
 }
 
 

@@ -34,6 +34,13 @@ extern "C" {
 
 typedef size_t cfft_size_t;        /* soi.h:220 */
 typedef void *soi_comm_t;          /* stands in for MPI_Comm (soi.h:238) */
+/* soi.h:227: one interleaved (re, im) pair of doubles.  C sees the C99 complex
+ * type the reference uses; C++ (no _Complex) a struct of the same layout. */
+#ifdef __cplusplus
+typedef struct { double re, im; } cfft_complex_t;
+#else
+typedef double _Complex cfft_complex_t;
+#endif
 
 typedef enum {
   SOI_PRECISION_FP64 = 0,          /* plain method, FP64 complex throughout        */
@@ -57,6 +64,19 @@ typedef struct {
   int rank;               /* soi.h:240, must be 0                                */
   cfft_size_t k;          /* soi.h:241, segments (S = k*P)                       */
   cfft_size_t N;          /* soi.h:242, transform length                         */
+  /* soi.h:243-251: the reference's host tables and work buffers.  Present so
+   * that its callers compile and run unchanged (test.c:409-420 frees them and
+   * sets them to NULL after every compute).  This library keeps its tables
+   * and buffers on the device, inside `plan`: set_default_soi_descriptor sets
+   * these to NULL, and nothing in the library reads, writes or frees them. */
+  cfft_complex_t *W_inv;
+  cfft_complex_t *w;
+  void *w_dup;            /* SIMDFPTYPE * in soi.h:245                           */
+  cfft_complex_t *gamma_tilde;
+  cfft_complex_t *alpha_tilde;
+  cfft_complex_t *beta_tilde;
+  cfft_complex_t *alpha_ghost;
+  int *delta, *epsilon;
   int n_mu;               /* soi.h:252, oversampling numerator                   */
   int d_mu;               /* soi.h:253, oversampling denominator                 */
   cfft_size_t B;          /* soi.h:254, window taps                              */
@@ -224,7 +244,7 @@ int soi_vlc_decompress_device(const int *words_dev, long stride_words, int len, 
  * static device array of 32 MiB of compressed words (plus 16 KiB of
  * per-chunk exponents and counts) that every GPU loading this library holds
  * until the process exits.  Limits: len a multiple of 16, nchunks <= 2047,
- * nchunks * soi_vlc_words(len, 0, 0) <= 8388608 (about 2.4M doubles in
+ * nchunks * soi_vlc_words(len, 0, 0) <= 8388608 (about 4.8M doubles in
  * total); larger requests return SOI_ERR_INVALID with a message on stderr.
  * The first call on each device looks up the array's device address
  * (cudaGetSymbolAddress), so make that first call before any stream capture.
@@ -234,7 +254,8 @@ int soi_vlc_decompress_device(const int *words_dev, long stride_words, int len, 
  * `stream`; the call returns without synchronising. */
 int soi_vlc_roundtrip_noalloc_device(const double *x_dev, double *out_dev, int len, int nchunks,
                                      void *stream);
-/* Words compress() writes for one chunk (pfft.c:397-402 sizing). */
+/* Words compress() writes for one chunk (pfft.c:397-402 sizing); -1 when the
+ * count does not fit in an int (len above ~613M doubles at full width). */
 int soi_vlc_words(int len, int e_max, int e_max_i);
 
 /* ---- learned window surrogate (no counterpart in the reference) --------- */

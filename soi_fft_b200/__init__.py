@@ -37,7 +37,13 @@ class SoiError(RuntimeError):
 
 class _Desc(ctypes.Structure):
     _fields_ = [("comm", ctypes.c_void_p), ("P", ctypes.c_int), ("rank", ctypes.c_int),
-                ("k", ctypes.c_size_t), ("N", ctypes.c_size_t), ("n_mu", ctypes.c_int),
+                ("k", ctypes.c_size_t), ("N", ctypes.c_size_t),
+                # soi.h:243-251, kept NULL (the library never touches them)
+                ("W_inv", ctypes.c_void_p), ("w", ctypes.c_void_p), ("w_dup", ctypes.c_void_p),
+                ("gamma_tilde", ctypes.c_void_p), ("alpha_tilde", ctypes.c_void_p),
+                ("beta_tilde", ctypes.c_void_p), ("alpha_ghost", ctypes.c_void_p),
+                ("delta", ctypes.POINTER(ctypes.c_int)), ("epsilon", ctypes.POINTER(ctypes.c_int)),
+                ("n_mu", ctypes.c_int),
                 ("d_mu", ctypes.c_int), ("B", ctypes.c_size_t), ("tau", ctypes.c_double),
                 ("sigma", ctypes.c_double), ("use_vlc", ctypes.c_int),
                 ("segmentBoundaries", ctypes.POINTER(ctypes.c_int)),

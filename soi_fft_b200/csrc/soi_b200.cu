@@ -1082,7 +1082,7 @@ int run_vlc(Plan &p, const Exec &ex)
                                                                       p.d_vlc_emax, p.d_vlc_words, p.vlc_stride,
                                                                       p.d_vlc_n);
     CK(cudaGetLastError());
-    vlc_decompress_kernel<double><<<gv, 256, vlc_decompress_smem(), st>>>(p.d_vlc_words, p.vlc_stride, len, nullptr,
+    vlc_decompress_kernel<double><<<gv, 256, vlc_decompress_smem(), st>>>(p.d_vlc_words, p.vlc_stride, len, 0,
                                                                           p.d_vlc_emax + ns, p.d_vlc_emax,
                                                                           (double *)T);
   } else {
@@ -1090,7 +1090,7 @@ int run_vlc(Plan &p, const Exec &ex)
                                                                      p.d_vlc_emax, p.d_vlc_words, p.vlc_stride,
                                                                      p.d_vlc_n);
     CK(cudaGetLastError());
-    vlc_decompress_kernel<float><<<gv, 256, vlc_decompress_smem(), st>>>(p.d_vlc_words, p.vlc_stride, len, nullptr,
+    vlc_decompress_kernel<float><<<gv, 256, vlc_decompress_smem(), st>>>(p.d_vlc_words, p.vlc_stride, len, 0,
                                                                          p.d_vlc_emax + ns, p.d_vlc_emax,
                                                                          (float *)T);
   }
@@ -1696,16 +1696,27 @@ int soi_mlp_adam_device(float *params, float *m, float *v, const float *grad, fl
   return SOI_OK;
 }
 
-int soi_vlc_words(int len, int e_max, int e_max_i)
+// Words compress() writes for one chunk of len doubles (pfft.c:397-402), in
+// 64 bits: 3.5 words per double at full width, so an int overflows past
+// ~613M doubles.
+static long long vlc_words_ll(long long len, int e_max, int e_max_i)
 {
   const int delta = e_max - e_max_i;
   const int i1 = (52 + 3 - 31) - delta, i2 = std::min(32, 52 + 3 - delta);
+  if (len < 0) return -1;
   if (i2 <= 0) return 0;
-  const int nb = (i1 > 0 ? i1 : 0) + i2;
-  const long long lanes = (long long)(len / 16) * nb;
+  const long long nb = (i1 > 0 ? i1 : 0) + i2;
+  const long long lanes = (len / 16) * nb;
   long long w = (lanes + 31) / 32 * 16;
-  w += ((long long)(len % 16) * nb + 31) / 32;
-  return (int)w;
+  w += ((len % 16) * nb + 31) / 32;
+  return w;
+}
+
+// The same count as an int, or -1 when it does not fit in one.
+int soi_vlc_words(int len, int e_max, int e_max_i)
+{
+  const long long w = vlc_words_ll(len, e_max, e_max_i);
+  return w > 2147483647LL ? -1 : (int)w;
 }
 
 int soi_vlc_max_exponent_device(const double *x, int len, int nchunks, int *e_max_out, void *stream)
@@ -1731,14 +1742,9 @@ int soi_vlc_decompress_device(const int *words, long stride_words, int len, int 
 {
   if (!words || !e_max_i || !out || len <= 0 || nchunks <= 0) return SOI_ERR_INVALID;
   if (len % 16) return SOI_ERR_UNSUPPORTED;
-  int *d_emax = nullptr;
-  CK(cudaMallocAsync(&d_emax, sizeof(int), (cudaStream_t)stream));
-  CK(cudaMemcpyAsync(d_emax, &e_max, sizeof(int), cudaMemcpyHostToDevice, (cudaStream_t)stream));
   dim3 g(64, (unsigned)nchunks);
-  vlc_decompress_kernel<<<g, 256, 0, (cudaStream_t)stream>>>(words, stride_words, len, nullptr, d_emax, e_max_i, out);
+  vlc_decompress_kernel<<<g, 256, 0, (cudaStream_t)stream>>>(words, stride_words, len, e_max, nullptr, e_max_i, out);
   CK(cudaGetLastError());
-  CK(cudaFreeAsync(d_emax, (cudaStream_t)stream));
-  CK(cudaStreamSynchronize((cudaStream_t)stream));
   return SOI_OK;
 }
 
@@ -1904,9 +1910,11 @@ extern "C" int soi_vlc_roundtrip_noalloc_device(const double *x_dev, double *out
 {
   if (!x_dev || !out_dev || len <= 0 || nchunks <= 0) return SOI_ERR_INVALID;
   if (len % 16) return SOI_ERR_UNSUPPORTED;
-  // worst case of compress(): every element at full width (56 bits)
-  const long long per_chunk = soi_vlc_words(len, 0, 0);
-  if (nchunks > kNoallocMaxChunks || per_chunk * nchunks > kNoallocWordInts) {
+  // worst case of compress(): every element at full width (56 bits), counted
+  // in 64 bits (len * 3.5 words does not fit an int past ~613M doubles)
+  const long long per_chunk = vlc_words_ll(len, 0, 0);
+  if (nchunks > kNoallocMaxChunks || per_chunk <= 0 || per_chunk > kNoallocWordInts ||
+      per_chunk * nchunks > kNoallocWordInts) {
     fprintf(stderr,
             "soi_vlc_roundtrip_noalloc_device: %d chunks of %d doubles need %lld scratch words; the static "
             "scratch holds %lld words in at most %d chunks\n",
@@ -1931,7 +1939,7 @@ extern "C" int soi_vlc_roundtrip_noalloc_device(const double *x_dev, double *out
   dim3 g(64, (unsigned)nchunks);
   vlc_compress_kernel<<<g, 256, 0, st>>>(x_dev, len, 0, g_max, e_max_i, words, (long)per_chunk, nwords);
   CK(cudaGetLastError());
-  vlc_decompress_kernel<<<g, 256, 0, st>>>(words, (long)per_chunk, len, nullptr, g_max, e_max_i, out_dev);
+  vlc_decompress_kernel<<<g, 256, 0, st>>>(words, (long)per_chunk, len, 0, g_max, e_max_i, out_dev);
   CK(cudaGetLastError());
   return SOI_OK;
 }

@@ -181,15 +181,15 @@ __global__ void vlc_compress_kernel(const X *x, int len, int e_max_host, const i
 }
 
 // compress.c:428-544 (vector body, :395-426 and :450-489), one chunk per
-// blockIdx.y; one thread per unit (lane L, block k of 32 fields).
+// blockIdx.y; one thread per unit (lane L, block k of 32 fields).  e_max =
+// *e_max_dev when given, else e_max_host; e_max_i[c] per chunk.
 // Y = double, or float for the split form (the decoded double rounded to float)
 template <typename Y>
-__global__ void vlc_decompress_kernel(const int *words, long stride, int len, const int *unused,
+__global__ void vlc_decompress_kernel(const int *words, long stride, int len, int e_max_host,
                                       const int *e_max_dev, const int *e_max_i, Y *out)
 {
-  (void)unused;
   const int c = blockIdx.y;
-  const int e_max = *e_max_dev;
+  const int e_max = e_max_dev ? *e_max_dev : e_max_host;
   const VlcBits b = vlc_bits(e_max, e_max_i[c]);
   Y *oc = out + (size_t)c * len;
   const uint32_t *wc = reinterpret_cast<const uint32_t *>(words + (size_t)c * stride);

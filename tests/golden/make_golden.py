@@ -29,7 +29,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("SOI_REFERENCE_TREE", "/root/reference")
+REF = os.environ.get("SOI_REFERENCE_TREE", "")
 
 
 def parse_vlc_vectors():
@@ -108,6 +108,8 @@ def soi_fixture():
 
 
 if __name__ == "__main__":
+    if not os.path.isfile(os.path.join(REF, "compress.c")):
+        sys.exit("set SOI_REFERENCE_TREE to the reference tree (the directory holding compress.c)")
     json.dump(vlc_fixture(), open(os.path.join(HERE, "vlc_compress_c.json"), "w"), indent=1)
     json.dump(soi_fixture(), open(os.path.join(HERE, "soi_small.json"), "w"), indent=1)
     print("wrote fixtures", file=sys.stderr)

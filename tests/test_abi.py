@@ -102,3 +102,29 @@ def test_factorised_window_equals_reference_window(N, S, n, d, B, tau, sigma):
                                             (32, 0, -60), (17, 3, 1)])
 def test_vlc_word_count_matches_oracle(ln, emax, emaxi):
     assert sb.lib().soi_vlc_words(ln, emax, emaxi) == oracle.vlc_words(ln, emax, emaxi)
+
+
+def test_vlc_words_reports_overflow_instead_of_wrapping():
+    L = sb.lib()
+    # 1.75 words per double at full width (56 bits): 2^30 doubles fit in an
+    # int count, 2^31 - 16 (3.76e9 words) do not
+    assert L.soi_vlc_words(1 << 29, 0, 0) == (1 << 29) // 16 * 28
+    assert L.soi_vlc_words(1 << 30, 0, 0) == (1 << 30) // 16 * 28
+    assert L.soi_vlc_words((1 << 31) - 16, 0, 0) == -1
+
+
+@pytest.mark.parametrize("ln,nchunks", [
+    ((1 << 31) - 16, 1),          # the word count overflows an int
+    ((1 << 31) - 16, 2047),
+    (1 << 30, 2),                 # fits an int per chunk; the product does not fit the scratch
+    (74896 + 16, 64),             # over the 8388608-word scratch by one group per chunk
+    (4793488 + 16, 1),
+    (16, 2048),                   # too many chunks
+])
+def test_noalloc_rejects_oversized_requests_before_touching_the_gpu(ln, nchunks):
+    L = sb.lib()
+    fn = L.soi_vlc_roundtrip_noalloc_device
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+    # non-null stand-in pointers: the size check comes before any device access,
+    # so without a GPU the call returns SOI_ERR_INVALID, not SOI_ERR_CUDA
+    assert fn(ctypes.c_void_p(256), ctypes.c_void_p(256), ln, nchunks, None) == 1

@@ -48,7 +48,7 @@ def test_oracle_vs_direct_fft(N, S):
     assert rel_l2(y, np.fft.fft(x)) < 1e-13
 
 
-needs_ref = pytest.mark.skipif(not oracle.ref_available(), reason="oracle/_ref not built (make -C oracle ref)")
+needs_ref = pytest.mark.skipif(not oracle.ref_available(), reason="oracle/_ref not built (make -C oracle ref REF=<reference tree>)")
 
 
 @needs_ref

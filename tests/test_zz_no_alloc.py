@@ -43,7 +43,11 @@ def test_noalloc_round_trip_matches_existing_entry_points_twice():
     L = sb.lib()
     L.soi_vlc_roundtrip_noalloc_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                                    ctypes.c_int, ctypes.c_void_p]
-    for call, (ln, nchunks, seed) in enumerate([(40960, 16, 1), (4096, 37, 2)]):
+    # two small calls, then the two capacity corners: the most chunks (2047,
+    # the per-chunk header full) and exactly the 8388608-word scratch
+    cases = [(40960, 16, 1), (4096, 37, 2), (16, 2047, 3), (74896, 64, 4)]
+    assert L.soi_vlc_words(74896, 0, 0) * 64 == 8388608
+    for call, (ln, nchunks, seed) in enumerate(cases):
         rng = np.random.default_rng(seed)
         x = rng.standard_normal((nchunks, ln)) * 2.0 ** rng.integers(-12, 12, size=(nchunks, 1))
         xd = torch.from_numpy(x).cuda()
@@ -64,4 +68,9 @@ def test_noalloc_rejects_requests_beyond_its_scratch():
     too_long = 1 << 23                       # 8M doubles in one chunk
     assert L.soi_vlc_roundtrip_noalloc_device(ptr(x), ptr(x), too_long, 1, None) == 1
     assert L.soi_vlc_roundtrip_noalloc_device(ptr(x), ptr(x), 16, 5000, None) == 1
+    # one past each capacity corner
+    assert L.soi_vlc_roundtrip_noalloc_device(ptr(x), ptr(x), 16, 2048, None) == 1
+    assert L.soi_vlc_roundtrip_noalloc_device(ptr(x), ptr(x), 74896, 65, None) == 1
+    assert L.soi_vlc_roundtrip_noalloc_device(ptr(x), ptr(x), 74896 + 16, 64, None) == 1
+    assert L.soi_vlc_roundtrip_noalloc_device(ptr(x), ptr(x), 1 << 30, 1, None) == 1
     assert L.soi_vlc_roundtrip_noalloc_device(ptr(x), ptr(x), 17, 1, None) == 2

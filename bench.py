@@ -49,7 +49,7 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = dict(N=1 << 29, S=128, n_mu=5, d_mu=4, B=72)
 METRIC = "GFLOP/s (5N log2 N) at N=2^29, split-FP32 vs plain FP64 GPU, at rel-L2 <=1e-6"
-CPU_SAMPLE_LOG2N = 24
+CPU_SAMPLE_LOG2N = 26
 
 # The two kernels of the split-precision path at this workload, their DRAM
 # traffic per launch as a multiple of the algorithmic bytes (dram__bytes_read
@@ -64,6 +64,18 @@ KERNELS = {
                "ncu at N=2^26, S=128 (same kernel instance), scaled by the units processed"),
     "stage2": ("k_stage2_ct (stage 2: M'-point four-step FFT + demodulation + discard)", 8724.6 / 4831.8,
                "ncu at N=2^28, S=64 (same M' tiles), scaled by the segments"),
+}
+
+
+# FP64 kernels of the configured plain workload (N = 2^28, S = 64): figures
+# from ncu captures of the same instances (stage 1 at N = 2^26, S = 64, whose
+# per-output behaviour does not depend on N; stage 2 at N = 2^26, S = 16, the
+# same M' = 2560 x 2048 tiles).
+FP64_PROFILE = {
+    "stage1": {"fp64_pipe_frac": 0.518, "traffic_ratio": 2.365 / 2.416,
+               "profile": "ncu --set full at N=2^26, S=64, same instance"},
+    "stage2": {"fp64_pipe_frac": 0.242, "traffic_ratio": 5.797 / 2.416,
+               "profile": "ncu --set full at N=2^26, S=16, same M' tiles"},
 }
 
 
@@ -87,6 +99,12 @@ def parse():
     ap.add_argument("--batch-chains", type=int, default=16)
     ap.add_argument("--vlc", action="store_true",
                     help="with the VLC round trip between the stages (use_vlc = 1, pfft.c:316-353,618-632)")
+    ap.add_argument("--precision", default="split", choices=["split", "fp64"],
+                    help="precision of the main leg (fp64: the plain method, for per-kernel profiling runs)")
+    ap.add_argument("--no-config2", action="store_true",
+                    help="skip the plain FP64 leg at N=2^28, S=64 (the configured FP64 workload)")
+    ap.add_argument("--ref-log2n", type=int, default=None,
+                    help="reference arm: transform size (default: the headline --log2n)")
     return ap.parse_args()
 
 
@@ -265,27 +283,30 @@ def make_signal(N, seed, device):
     return x
 
 
-def cpu_baseline(log2n, S, steps, threads=None, bounded=True):
+def cpu_baseline(log2n, S, repeat=4, threads=None, ranks=1):
     """The reference's compute_soi compiled from its own sources (oracle/_ref),
-    1 rank x T OpenMP threads, on a bounded sample of the workload."""
+    `ranks` forked ranks x T OpenMP threads each, best of `repeat` runs as the
+    reference's driver reports (test.c:217, REPEAT = 4)."""
     from oracle import oracle
     import numpy as np
     if not oracle.ref_available():
         return None
     N = 1 << log2n
     ncpu = os.cpu_count() or 8
+    k = S // ranks
     ntg = min(S // 4, 8)
-    T = threads or max(ntg, ncpu // ntg * ntg)
+    T = threads or max(ntg, (ncpu // ranks) // ntg * ntg)
     r = np.random.default_rng(1)
     x = r.standard_normal(N) + 1j * r.standard_normal(N)
-    _, best, times = oracle.run_reference(x, 1, S, threads=T, repeat=steps, return_times=True)
-    mean = statistics.mean(times)
-    return {"value": flop(N) / mean / 1e9, "best_value": flop(N) / best / 1e9, "unit": "GFLOP/s",
-            "cores": T, "kind": "reference",
+    _, best, times = oracle.run_reference(x, ranks, k, threads=T, repeat=repeat, return_times=True)
+    del x
+    return {"value": flop(N) / best / 1e9, "mean_value": flop(N) / statistics.mean(times) / 1e9,
+            "unit": "GFLOP/s", "cores": ranks * T, "kind": "reference",
             "sample": "reference compute_soi (pfft.c + parallel_filter_subsampling.cpp built here, "
                       "DFTI backed by the oracle FFT, not MKL) at N=2^%d, S=%d, mu=5/4, B=72, FP64, "
-                      "1 rank x %d threads, mean of %d runs" % (log2n, S, T, steps),
-            "seconds_per_transform": mean}
+                      "%d rank%s x %d threads on %d host cores, best of %d runs (test.c:217)"
+                      % (log2n, S, ranks, "s" if ranks > 1 else "", T, ncpu, repeat),
+            "seconds_per_transform": best, "seconds_all": times}
 
 
 # ------------------------------------------------------------- reference ---
@@ -296,20 +317,40 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    log2n = min(args.log2n, CPU_SAMPLE_LOG2N)
-    res = cpu_baseline(log2n, args.segments, args.steps + args.warmup)
+    # the headline transform itself (N = 2^29, S = 128: ~14 s per run on 16
+    # host threads); the reference's driver times REPEAT = 4 runs and reports
+    # the best (test.c:217), so the arm runs 1 + min(steps, 3) and reports the
+    # best of the runs after the first
+    log2n = args.ref_log2n or args.log2n
+    repeat = 1 + max(1, min(args.steps, 3))
+    res = cpu_baseline(log2n, args.segments, repeat=repeat)
     if res is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/soi_ref_run is not built"}))
         return
-    line = {"metric": METRIC, "value": res["value"], "unit": "GFLOP/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": res["seconds_per_transform"] * 1e3, "higher_is_better": True,
+    timed_runs = res["seconds_all"][1:] or res["seconds_all"]
+    best = min(timed_runs)
+    N = 1 << log2n
+    value = flop(N) / best / 1e9
+    cb = {k: res[k] for k in ("unit", "cores", "kind")}
+    cb.update(value=value, sample="%s; the first run untimed" % res["sample"])
+    # the reference's own CPU configuration (N = 2^20, 8 ranks x 2 threads, best of 4)
+    try:
+        c1 = cpu_baseline(20, 8, repeat=4, threads=2, ranks=8)
+        config1 = {k: c1[k] for k in ("value", "unit", "cores", "kind", "sample")} if c1 else None
+    except Exception as e:
+        config1 = {"error": str(e)[:200]}
+    line = {"metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": args.gpus,
+            "steps": len(timed_runs), "warmup": 1,
+            "ms_per_step": best * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
             "data": "synthetic: seeded i.i.d. complex Gaussian",
-            "config": {"workload": "SOI FFT, reference CPU path, bounded sample N=2^%d of N=2^%d" % (log2n, args.log2n),
-                       "N": 1 << log2n, "S": args.segments, "mu": "5/4", "B": 72},
-            "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
-            "e2e": {"value": res["value"], "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "config": {"workload": "SOI FFT, reference CPU path (FP64), N=2^%d, S=%d, mu=5/4, B=72"
+                                   % (log2n, args.segments),
+                       "N": N, "S": args.segments, "mu": "5/4", "B": 72,
+                       "same_size_as_gpu_arm": log2n == args.log2n},
+            "cpu_baseline": cb,
+            "cpu_config1": config1,
+            "e2e": {"value": value, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
@@ -330,7 +371,10 @@ def run_ours(args):
     torch.cuda.set_stream(stream)
 
     x128 = make_signal(N, 1234, dev)
-    x32 = x128.to(torch.complex64)
+    split = args.precision == "split"
+    PREC = sb.PRECISION_SPLIT_FP32 if split else sb.PRECISION_FP64
+    ELEM = 8 if split else 16
+    x32 = x128.to(torch.complex64) if split else x128
 
     def new_desc(prec):
         d = sb.SoiDescriptor(N=N, precision=prec, device=local, stream=stream.cuda_stream, use_vlc=int(args.vlc))
@@ -374,8 +418,9 @@ def run_ours(args):
         d.set_timing(False)
         return e0.elapsed_time(e1), st
 
-    # ---- split precision, device-resident (the headline `value`)
-    d32 = new_desc(sb.PRECISION_SPLIT_FP32)
+    # ---- split precision, device-resident (the headline `value`; with
+    # --precision fp64 the plain method in its place, for profiling runs)
+    d32 = new_desc(PREC)
     y32 = torch.empty_like(x32)
     peaks = measured_peaks()
     launches_per_step = d32.kernels_per_compute() if hasattr(d32, "kernels_per_compute") else None
@@ -403,9 +448,9 @@ def run_ours(args):
     # uploads its input and downloads its result.  The streamed call overlaps
     # one step's upload with the previous step's kernels and download; the
     # one-at-a-time call (compute_soi's form) is reported beside it.
-    h_in = torch.empty(N, dtype=torch.complex64, pin_memory=True)
+    h_in = torch.empty(N, dtype=x32.dtype, pin_memory=True)
     h_in.copy_(x32)
-    h_out = torch.empty(N, dtype=torch.complex64, pin_memory=True)
+    h_out = torch.empty(N, dtype=x32.dtype, pin_memory=True)
     e2e_steps = max(3, min(args.steps, 10))
     hi, ho = h_in.numpy(), h_out.numpy()
     d32.compute_stream([hi], [ho])
@@ -430,7 +475,7 @@ def run_ours(args):
 
     # ---- plain FP64 method at the same N
     fp64 = None
-    if not args.no_fp64:
+    if not args.no_fp64 and split:
         d64 = new_desc(sb.PRECISION_FP64)
         y64 = torch.empty_like(x128)
         ms64, _ = timed(d64, x128, y64, max(2, min(args.steps, 5)), 2)
@@ -444,12 +489,14 @@ def run_ours(args):
     # ---- roofline of the dominant kernel.  Both stages move the same
     # algorithmic bytes: stage 1 reads the N inputs and writes the S*M'
     # transposed values, stage 2 reads those and writes the N outputs.
-    geom = sb.plan_geometry(N, S, sb.PRECISION_SPLIT_FP32)
-    alg_bytes = (N + geom["M_hat"] * S) * 8
+    geom = sb.plan_geometry(N, S, PREC)
+    alg_bytes = (N + geom["M_hat"] * S) * ELEM
     hbm = peaks["hbm_gbs"] if peaks else 6650.0
     dom_ms = max(stage1, stage2)
     achieved = alg_bytes / (dom_ms / 1e3) / 1e9
     name, traffic_ratio, traffic_source = KERNELS["stage1" if stage1 >= stage2 else "stage2"]
+    if not split or N != 1 << 29 or S != 128:
+        traffic_ratio, traffic_source = None, None          # the captures cover the headline instance only
     roofline = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_source": "measured" if peaks else "fallback",
                 "traffic": traffic_ratio * alg_bytes if traffic_ratio else None,
@@ -458,10 +505,47 @@ def run_ours(args):
                 "stage1_ms": stage1, "stage2_ms": stage2, "vlc_ms": vlc_ms if args.vlc else None,
                 "pipeline_achieved_gbs": 2 * alg_bytes / (ms_step / 1e3) / 1e9}
 
+    # ---- the configured plain-FP64 workload: N = 2^28 complex128, S = 64,
+    # Gaussian + 64 tones; per-kernel CUDA-event times and HBM GB/s against
+    # the measured peak (algorithmic bytes: each kernel reads and writes
+    # (1 + mu) N complex128 values between them), accuracy against cuFFT Z2Z
+    config2 = None
+    if not args.no_config2 and split and not args.no_fp64:
+        del X
+        N2, S2 = 1 << 28, 64
+        x2 = make_signal(N2, 2828, dev)
+        d2 = sb.SoiDescriptor(N=N2, precision=sb.PRECISION_FP64, device=local, stream=stream.cuda_stream).init(S2)
+        y2 = torch.empty_like(x2)
+        k2 = max(3, min(args.steps, 10))
+        ms2, _ = timed(d2, x2, y2, k2, 3)
+        ms2 = max_over_ranks_(ms2) / k2
+        _, st2 = timed(d2, x2, y2, k2, 0, per_stage=True)
+        g2 = sb.plan_geometry(N2, S2, sb.PRECISION_FP64)
+        b2 = (N2 + g2["M_hat"] * S2) * 16
+        X2 = torch.fft.fft(x2)
+        acc2 = float(torch.linalg.norm(y2 - X2) / torch.linalg.norm(X2))
+        del X2
+        kern = {}
+        for key, kname in (("stage1", "k_conv_sfft_tS<double, 5, 4, 8, 8, 512, false> (convolution + 64-point FFTs "
+                                       "+ transposed store)"),
+                           ("stage2", "k_stage2_ct<double, 10, 16, 16, 8, 16, 16, 256, 2, 2> (M'-point four-step "
+                                      "FFT + demodulation + discard)")):
+            kms = statistics.mean(t[key + "_ms"] for t in st2)
+            gbs = b2 / (kms / 1e3) / 1e9
+            kern[key] = dict(kernel=kname, ms=kms, algorithmic_bytes=b2, achieved_gbs=gbs, peak_gbs=hbm,
+                             frac_hbm=gbs / hbm, **FP64_PROFILE.get(key, {}))
+            if "traffic_ratio" in kern[key]:
+                kern[key]["traffic"] = kern[key]["traffic_ratio"] * b2
+        config2 = {"workload": "plain FP64, N=2^28 complex128, S=64, mu=5/4, B=72, Gaussian + 64 tones",
+                   "value": world * flop(N2) / (ms2 / 1e3) / 1e9, "unit": "GFLOP/s", "ms_per_step": ms2,
+                   "steps": k2, "rel_l2_vs_fp64_direct_fft": acc2, "kernels": kern}
+        d2.free()
+        del x2, y2
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cpu = cpu_baseline(min(args.log2n, CPU_SAMPLE_LOG2N), S, 2)
+            cpu = cpu_baseline(min(args.log2n, CPU_SAMPLE_LOG2N), S, repeat=4)
         except Exception as e:  # the checker failing must not hide the measurement
             cpu = {"error": str(e)[:200]}
         if cpu and "value" in cpu:
@@ -470,21 +554,24 @@ def run_ours(args):
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32" if split else "f64",
                 "data": "synthetic: seeded complex Gaussian + 64 tones, amplitudes log-uniform [1e-6, 1]",
-                "config": {"workload": "SOI FFT split-precision, N=2^%d complex64, S=%d, mu=5/4, B=72%s"
-                                       % (args.log2n, S, ", VLC round trip" if args.vlc else ""),
+                "config": {"workload": "SOI FFT %s, N=2^%d %s, S=%d, mu=5/4, B=72%s"
+                                       % ("split-precision" if split else "plain FP64", args.log2n,
+                                          "complex64" if split else "complex128", S,
+                                          ", VLC round trip" if args.vlc else ""),
                            "use_vlc": bool(args.vlc),
-                           "N": N, "S": S, "mu": "5/4", "B": 72, "precision": "split_fp32",
-                           "l2": "inputs (%d MiB) larger than L2 (126 MB), no flush" % (N * 8 >> 20),
+                           "N": N, "S": S, "mu": "5/4", "B": 72, "precision": "split_fp32" if split else "fp64",
+                           "l2": "inputs (%d MiB) larger than L2 (126 MB), no flush" % (N * ELEM >> 20),
                            "parallelism": "replicas x%d" % world},
                 "accuracy_vs_fp64_direct_fft": acc32,
                 "fp64_plain": fp64,
+                "fp64_config2": config2,
                 "split_over_fp64": (value / fp64["value"]) if fp64 else None,
                 "roofline": roofline,
                 "cpu_baseline": cpu,
                 "e2e": {"value": e2e_value, "unit": "GFLOP/s", "ms_per_step": e2e_ms,
-                        "h2d_bytes_per_step": N * 8, "d2h_bytes_per_step": N * 8,
+                        "h2d_bytes_per_step": N * ELEM, "d2h_bytes_per_step": N * ELEM,
                         "api": "soi_compute_stream_status, %d transforms per call, pinned host buffers" % e2e_steps,
                         "matches_device_result": e2e_matches,
                         "one_at_a_time": {"api": "soi_compute_oop_status", "ms_per_step": single_ms,

@@ -20,6 +20,7 @@
 #include "vlc_kernels.cuh"
 #include "stage2_fast.cuh"
 #include "stage1_fast.cuh"
+#include "stage1_tc.cuh"
 #include "mlp_kernels.cuh"
 
 using namespace soi;
@@ -64,6 +65,7 @@ struct Plan {
   int f2_grid = 0;
   size_t f2_smem = 0;
   int discard = 1;             // drop consumed intermediate lines from L2
+  int amp_keep = 0;            // demodulation amplitude loads hint L2 evict_last
   int wait_extra = 0;          // failure test: pass-2 waits for a count that never comes
   void *d_amp = nullptr;            // [M1][M2] real demodulation amplitude, pass-2 store order
   void *d_ctw1 = nullptr, *d_ctw2 = nullptr;   // tile-FFT twiddles of the two passes, warp read order
@@ -84,6 +86,9 @@ struct Plan {
   int knob_s1_nt = -1;              // 256 or 512 threads for the compile-time-S stage 1
   int knob_s2 = -1;                 // 1 persistent stage 2, 0 two-kernel stage 2
   int knob_s1_bulk = -1;            // 1/0: stage-1 staging by bulk copies or cp.async
+  // tensor-core stage 1 (split form, n = 5, d = 4, S in {32, 64, 128}, B <= 72 taps)
+  int s1_tc = 0;
+  void *d_btc = nullptr;            // [S][16 rows][72 taps] TF32 hi/lo filter, the MMA's B layout
   bool timing = false;
   cudaEvent_t ev[5] = {};
   float ms[4] = {0, 0, 0, 0};
@@ -521,6 +526,7 @@ int setup_s2ct(Plan &p, int idx)
   int rc = p.prec == SOI_PRECISION_FP64 ? build_ct_tables<double>(p, c) : build_ct_tables<float>(p, c);
   if (rc) return rc;
   p.discard = env_int("SOI_STAGE2_DISCARD", 1);
+  p.amp_keep = env_int("SOI_STAGE2_AMP_KEEP", 0) ? 1 : 0;
   // failure-detection test only: every pass-2 task then waits for one more
   // pass-1 completion than exists, runs out its iteration limit and the
   // compute returns SOI_ERR_TIMEOUT
@@ -539,6 +545,7 @@ int launch_s2ct(Plan &p, const Exec &ex)
   a.discard = p.discard;
   a.wait_extra = p.wait_extra;
   a.tail = p.f2_tail;
+  a.amp_keep = p.amp_keep;
   a.err = (int *)ex.sync; a.counter = ex.sync + 1; a.done1 = ex.sync + 2;
   // counters restart; the error flag stays set until the owner clears it
   CK(cudaMemsetAsync(ex.sync + 1, 0, (size_t)(a.S + 1) * sizeof(unsigned int), ex.st));
@@ -702,8 +709,82 @@ void plan_stage1_staged(Plan &p)
   }
 }
 
+// ---- tensor-core stage 1 --------------------------------------------------
+
+constexpr int kTcKP = 72;      // taps of the compiled instances (B <= 72, zero beyond B)
+
+// The tensor-core kernel applies to the split form with n = 5, d = 4, S in
+// {32, 64, 128}, at most 72 taps and whole 32-group tiles; SOI_STAGE1_TC=1
+// selects it (the packed-FMA kernel measured faster, so it is off by default).
+bool tc_available(const Plan &p)
+{
+  if (p.prec != SOI_PRECISION_SPLIT_FP32 || p.nmu != 5 || p.dmu != 4) return false;
+  if (!(p.S == 32 || p.S == 64 || p.S == 128)) return false;
+  if ((size_t)p.atap * 4 > (size_t)kTcKP || p.J % 32 || p.J < 64) return false;
+  return true;
+}
+
+// x rounded to 11 significant bits (TF32), ties away from zero like cvt.rna
+long double tf32_round(long double x)
+{
+  if (x == 0) return 0;
+  const int e = ilogbl(x);
+  const long double sc = ldexpl(1.0L, 10 - e);
+  return roundl(x * sc) / sc;
+}
+
+// B operand of every column: rows n = theta + 5*t' (t' = 0: F_hi, 1: F_lo;
+// rows 10..15 zero) by KP taps q, K-major core matrices of 8 rows x 4 taps:
+// byte offset (n/8)*(KP/4)*128 + (q/4)*128 + (n%8)*16 + (q%4)*4 within the
+// column's 64*KP bytes.  F[q][theta][s] is the long-double filter tap q.
+std::vector<float> tc_filter_table(const Plan &p, const std::vector<long double> &filt)
+{
+  const int KP = kTcKP, NA = KP / 4;
+  std::vector<float> t((size_t)p.S * 16 * KP, 0.0f);
+  for (size_t s = 0; s < p.S; ++s)
+    for (int th = 0; th < p.nmu; ++th)
+      for (int q = 0; q < KP && (size_t)q < p.B; ++q) {
+        const long double F = filt[((size_t)q * p.nmu + th) * p.S + s];
+        const long double hi = tf32_round(F), lo = tf32_round(F - hi);
+        for (int tp = 0; tp < 2; ++tp) {
+          const int n = th + 5 * tp;
+          const size_t off = (size_t)(n / 8) * NA * 32 + (size_t)(q / 4) * 32 + (n % 8) * 4 + (q % 4);
+          t[s * 16 * KP + off] = (float)(tp ? lo : hi);
+        }
+      }
+  return t;
+}
+
+template <int R0, int R1>
+int launch_tc_t(Plan &p, const Exec &ex)
+{
+  using Gm = TcGeom<R0, R1, kTcKP>;
+  Conv2Args a;
+  memset(&a, 0, sizeof a);
+  a.alpha = ex.in; a.T = ex.T; a.seg_lo = ex.lo; a.seg_hi = ex.hi; a.phase = p.d_phase; a.twS = p.d_twS;
+  a.M = (long long)p.M; a.Mh = (long long)p.Mh; a.J = (long long)p.J;
+  a.S = (int)p.S; a.d = p.dmu; a.atap = p.atap; a.JT = Gm::JT;
+  a.err = (int *)ex.sync;
+  auto kern = k_conv_sfft_tc<R0, R1, kTcKP>;
+  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Gm::SMEM));
+  kern<<<(unsigned)(p.J / Gm::JT), Gm::NT, Gm::SMEM, ex.st>>>(a, (const float *)p.d_btc);
+  CK(cudaGetLastError());
+  return SOI_OK;
+}
+
+int launch_tc(Plan &p, const Exec &ex)
+{
+  switch (p.S) {
+    case 32: return launch_tc_t<4, 8>(p, ex);
+    case 64: return launch_tc_t<8, 8>(p, ex);
+    case 128: return launch_tc_t<8, 16>(p, ex);
+  }
+  return SOI_ERR_UNSUPPORTED;
+}
+
 int run_stage1(Plan &p, const Exec &ex)
 {
+  if (p.s1_tc) return launch_tc(p, ex);
   if (p.s1fast) return launch_conv2(p, ex);
   return p.prec == SOI_PRECISION_FP64 ? launch_conv_r<double>(p, ex) : launch_conv_r<float>(p, ex);
 }
@@ -793,6 +874,10 @@ int build_tables(Plan &p)
       }
     if ((rc = upload(&p.d_filt2, f2.data(), f2.size() * sizeof(R)))) return rc;
   }
+  if (p.s1_tc) {
+    std::vector<float> bt = tc_filter_table(p, filt);
+    if ((rc = upload(&p.d_btc, bt.data(), bt.size() * sizeof(float)))) return rc;
+  }
   if ((rc = upload(&p.d_phase, ph.data(), ph.size() * sizeof(R)))) return rc;
   if ((rc = upload(&p.d_winv, wi.data(), wi.size() * sizeof(R)))) return rc;
   std::vector<R> tS = roots_table<R>((long long)p.S), t1 = roots_table<R>(p.M1), t2 = roots_table<R>(p.M2);
@@ -830,7 +915,7 @@ void free_plan(Plan *p)
   cudaSetDevice(p->device);
   void *bufs[] = { p->d_filt, p->d_phase, p->d_twS, p->d_tw1, p->d_tw2, p->d_winv, p->d_wsmall,
                    p->d_permS, p->d_perm1, p->d_perm2, p->d_xlo, p->d_xhi, p->d_T, p->d_io, p->d_io2,
-                   p->d_vlc_words, p->d_vlc_n, p->d_vlc_emax, p->d_sync, p->d_filt2, p->d_amp, p->d_dlo, p->d_dhi, p->d_ph2, p->d_ctw1, p->d_ctw2, p->d_base1, p->d_step1 };
+                   p->d_vlc_words, p->d_vlc_n, p->d_vlc_emax, p->d_sync, p->d_filt2, p->d_amp, p->d_dlo, p->d_dhi, p->d_ph2, p->d_ctw1, p->d_ctw2, p->d_base1, p->d_step1, p->d_btc };
   for (void *b : bufs) if (b) cudaFree(b);
   for (auto &e : p->ev) if (e) cudaEventDestroy(e);
   for (auto &e : p->sev) if (e) cudaEventDestroy(e);
@@ -867,6 +952,7 @@ int plan_geometry(const soi_desc_t *d, size_t k, Plan &p)
   p.JT = (int)jt;
   p.smem1 = (size_t)p.nmu * p.JT * p.pitch * p.elem + p.S * (p.elem + sizeof(int));
   plan_stage1_staged(p);
+  p.s1_tc = tc_available(p) && env_int("SOI_STAGE1_TC", 0) == 1 ? 1 : 0;
   const int ict = pick_s2ct(p);
   if (ict >= 0) {
     p.f2_variant = ict;

@@ -101,9 +101,31 @@ struct S2ArgsCT {
   int tma;                    // 1: pass-1 tiles come by tensor copy (the map in the launch's second argument)
   int wait_extra;             // 0; a test sets 1 to make every pass-2 wait run out
   int tail;                   // pass-2 tasks that end a block after its interleaved part (0 .. M1/C)
+  int amp_keep;               // 1: amp loads carry an L2 evict_last hint
   unsigned int *counter, *done1;
   int *err;
 };
+
+// a read-only load with an L2 eviction-priority hint (createpolicy); used
+// to keep a table that every segment re-reads resident in L2
+__device__ __forceinline__ float ldg_hint(const float *p, unsigned long long pol)
+{
+  float v;
+  asm volatile("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ double ldg_hint(const double *p, unsigned long long pol)
+{
+  double v;
+  asm volatile("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ unsigned long long l2_evict_last_policy()
+{
+  unsigned long long pol;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
 
 template <typename V>
 __device__ __forceinline__ V two_level(const double2 *lo, const double2 *hi, int bits, int e)
@@ -140,7 +162,7 @@ struct NoPre {};
 // k1_0 + C-1 own amp[(k1_0*M2 + pos*C) + col], so that a warp's loads (8
 // consecutive butterflies x C rows) are one cache line each
 template <typename V, int M1, int M2, int C, int RL, bool BATCH> struct EmitRowsCT {
-  V *oseg; int k1_0; const V *ph1; const S2ArgsCT *a;
+  V *oseg; int k1_0; const V *ph1; const S2ArgsCT *a; unsigned long long pol;
   __device__ __forceinline__ NoPre prepare(int, int, int) const { return NoPre{}; }
   template <int RLx> __device__ __forceinline__ void run(int col, int fbase, int fstep, V *v, NoPre, int blk) const
   {
@@ -158,7 +180,7 @@ template <typename V, int M1, int M2, int C, int RL, bool BATCH> struct EmitRows
 #pragma unroll
       for (int j = 0; j < RL; ++j) {
         const int pos = blk + fstep * j;
-        w[j] = cscale(cmul(p1, __ldg(ph2 + pos)), __ldg(amp + pos * C));
+        w[j] = cscale(cmul(p1, __ldg(ph2 + pos)), (a->amp_keep ? ldg_hint(amp + pos * C, pol) : __ldg(amp + pos * C)));
       }
 #pragma unroll
       for (int j = 0; j < RL; ++j) {
@@ -172,7 +194,7 @@ template <typename V, int M1, int M2, int C, int RL, bool BATCH> struct EmitRows
       for (int j = 0; j < RL; ++j) {
         const int pos = blk + fstep * j;
         const int k = k1 + M1 * (fbase + fstep * j);
-        const V w = cscale(cmul(p1, __ldg(ph2 + pos)), __ldg(amp + pos * C));
+        const V w = cscale(cmul(p1, __ldg(ph2 + pos)), (a->amp_keep ? ldg_hint(amp + pos * C, pol) : __ldg(amp + pos * C)));
         if (k < M) stcs(oseg + k, cmul(v[j], w));
       }
     }
@@ -253,6 +275,7 @@ __global__ void __launch_bounds__(NT, MINB) k_stage2_ct(S2ArgsCT a, const __grid
     if (c1 > c0) { kind = 1; seg = blk + 1; tile = c0; }
     else { kind = 2; seg = blk; tile = r - c0; }
   };
+  const unsigned long long amp_pol = l2_evict_last_policy();
   unsigned int next = 0;
   // thread 0: take the claimed task, claim the one after it, and for a
   // pass-2 task wait (bounded) until its segment's pass 1 is complete; the
@@ -372,7 +395,8 @@ __global__ void __launch_bounds__(NT, MINB) k_stage2_ct(S2ArgsCT a, const __grid
         constexpr int nlines = C * M2 * G::E / 128;
         for (int l = tid; l < nlines; l += NT) discard_l2_line(base + l * 128);
       }
-      EmitRowsCT<V, M1, M2, C, RLB, (MINB <= 2)> e{ reinterpret_cast<V *>(a.out) + (size_t)(a.seg_lo + seg) * a.M, k1_0, s_tab, &a };
+      EmitRowsCT<V, M1, M2, C, RLB, (MINB <= 2)> e{ reinterpret_cast<V *>(a.out) + (size_t)(a.seg_lo + seg) * a.M, k1_0, s_tab, &a,
+                                                    amp_pol };
       tile_fft_ct<V, B0, B1, B2, C, 1, G::PS2, NT>(buf, reinterpret_cast<const V *>(a.tw2), e);
       if (tid == 0) take(slot ^ 1);                           // after thread 0's own stores
     }

@@ -121,6 +121,16 @@ void parallel_filter_subsampling(soi_desc_t *desc, void *alpha_dt);
 /* Device inputs (device_ptr = 1) must start on a 16-byte boundary (memory
  * from cudaMalloc does); a misaligned input returns SOI_ERR_INVALID. */
 int soi_init_status(soi_desc_t *desc, soi_comm_t comm, cfft_size_t k);
+/* init_soi_descriptor with a caller's window in place of the analytic one
+ * (pfft.c:42-82): y_time[(kk*n_mu + theta)*k + s] is the real window y(t) at
+ * t = theta*d_mu/n_mu - kk - s/k + (B - d_mu)/2 for kk < B, theta < n_mu,
+ * s < k (the points where the reference evaluates w_f), and y_freq[j] is
+ * its Fourier transform at xi = j/M - 1/2, j = 0 .. M/2 (M = N/k; the
+ * transform is even, and must be positive there: the demodulation divides
+ * by it, SOI_ERR_INVALID otherwise).  tau and sigma are not used.  No
+ * counterpart in the reference. */
+int soi_init_window_status(soi_desc_t *desc, soi_comm_t comm, cfft_size_t k, const double *y_time,
+                           const double *y_freq);
 int soi_compute_status(soi_desc_t *desc, void *alpha_dt);
 /* Out-of-place compute_soi: `in` (N inputs) is left untouched, `out`
  * receives the N outputs; both host or both device memory per device_ptr.
@@ -272,6 +282,22 @@ int soi_mlp_grad_device(const float *params, const float *x, const float *y, int
                         void *stream);
 /* one Adam step (beta1 0.9, beta2 0.999, eps 1e-8) at 1-based step count */
 int soi_mlp_adam_device(float *params, float *m, float *v, const float *grad, float lr, int step, void *stream);
+
+/* ---- learned window proposer (no counterpart in the reference) ---------- */
+
+/* A 2-64-64-32 GELU MLP (FP32) mapping (mu, log10 target error), normalised by
+ * soi_fft_b200/window_cheb.py, to 32 Chebyshev coefficients of a window's
+ * frequency-response profile.  Layout W1[64][2] b1[64] W2[64][64] b2[64]
+ * W3[32][64] b3[32].  Device pointers. */
+int soi_wmlp_param_count(void);
+/* y[i][0..32) = MLP(x[i][0..2)) for i < n */
+int soi_wmlp_forward_device(const float *params, const float *x, float *y, int n, void *stream);
+/* grad = d/dparams of mean((MLP(x) - y)^2) over the n x 32 outputs, loss = that mean */
+int soi_wmlp_grad_device(const float *params, const float *x, const float *y, int n, float *grad, float *loss,
+                         void *stream);
+/* one Adam step (beta1 0.9, beta2 0.999, eps 1e-8) over `count` parameters */
+int soi_adam_device(float *params, float *m, float *v, const float *grad, int count, float lr, int step,
+                    void *stream);
 
 /* ---- host-side tables (no GPU needed) ---------------------------------- */
 

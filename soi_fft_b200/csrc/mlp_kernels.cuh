@@ -156,4 +156,148 @@ __global__ void mlp_adam_kernel(float *params, float *m, float *v, const float *
   }
 }
 
+// ---- the window proposer: an IN-64-64-OUT GELU MLP ------------------------
+//
+// Maps (oversampling mu, log10 of the target error; normalised on the host)
+// to OUT = 32 Chebyshev coefficients of a window's frequency-response profile
+// (soi_fft_b200/window_cheb.py).  Same GELU, layer width and Adam as the
+// surrogate above; the loss is the mean squared error over samples and
+// outputs.  Parameter layout: W1[64][IN] b1[64] W2[64][64] b2[64] W3[OUT][64]
+// b3[OUT].  No counterpart in the reference.
+namespace wmlp {
+
+constexpr int H = 64;
+template <int IN, int OUT> struct Dims {
+  static constexpr int W1 = 0, B1 = W1 + H * IN, W2 = B1 + H, B2 = W2 + H * H, W3 = B2 + H, B3 = W3 + OUT * H,
+                       P = B3 + OUT;
+};
+constexpr int kIn = 2, kOut = 32;
+constexpr int kParams = Dims<kIn, kOut>::P;
+constexpr int kBlock = 32;           // samples per block of the gradient kernel (one warp)
+
+template <int IN, int OUT>
+__device__ __forceinline__ void forward_one(const float *__restrict__ p, const float *x, float *z1, float *h1,
+                                            float *z2, float *h2, float *out)
+{
+  using G = Dims<IN, OUT>;
+  for (int j = 0; j < H; ++j) {
+    float s = __ldg(p + G::B1 + j);
+#pragma unroll
+    for (int i = 0; i < IN; ++i) s = fmaf(__ldg(p + G::W1 + j * IN + i), x[i], s);
+    z1[j] = s;
+    h1[j] = gelu_f(s, nullptr);
+  }
+  for (int j = 0; j < H; ++j) {
+    float s = __ldg(p + G::B2 + j);
+    for (int i = 0; i < H; ++i) s = fmaf(__ldg(p + G::W2 + j * H + i), h1[i], s);
+    z2[j] = s;
+    h2[j] = gelu_f(s, nullptr);
+  }
+  for (int o = 0; o < OUT; ++o) {
+    float s = __ldg(p + G::B3 + o);
+    for (int i = 0; i < H; ++i) s = fmaf(__ldg(p + G::W3 + o * H + i), h2[i], s);
+    out[o] = s;
+  }
+}
+
+// y[n][OUT] = MLP(x[n][IN])
+template <int IN, int OUT>
+__global__ void forward_kernel(const float *params, const float *x, float *y, int n)
+{
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    float z1[H], h1[H], z2[H], h2[H], o[OUT];
+    forward_one<IN, OUT>(params, x + (size_t)s * IN, z1, h1, z2, h2, o);
+    for (int k = 0; k < OUT; ++k) y[(size_t)s * OUT + k] = o[k];
+  }
+}
+
+// Gradient of mean((MLP(x) - y)^2) over n samples and OUT outputs,
+// accumulated into grad and loss (both zeroed by the caller).  One block of
+// kBlock samples: forward and backward per thread, weight gradients reduced
+// over the block's samples through shared memory.
+template <int IN, int OUT>
+__global__ void __launch_bounds__(kBlock) grad_kernel(const float *params, const float *x, const float *y, int n,
+                                                      float *grad, float *loss)
+{
+  using G = Dims<IN, OUT>;
+  __shared__ float s_x[kBlock][IN];
+  __shared__ float s_h1[kBlock][H + 1];
+  __shared__ float s_h2[kBlock][H + 1];
+  __shared__ float s_d1[kBlock][H + 1];
+  __shared__ float s_d2[kBlock][H + 1];
+  __shared__ float s_d3[kBlock][OUT + 1];
+  const int t = threadIdx.x;
+  const int s = blockIdx.x * kBlock + t;
+  const bool valid = s < n;
+  const float scale = 2.f / ((float)n * (float)OUT);
+  {
+    float xin[IN];
+    for (int i = 0; i < IN; ++i) xin[i] = valid ? x[(size_t)s * IN + i] : 0.f;
+    for (int i = 0; i < IN; ++i) s_x[t][i] = xin[i];
+    float z1[H], h1[H], z2[H], h2[H], o[OUT];
+    forward_one<IN, OUT>(params, xin, z1, h1, z2, h2, o);
+    float l = 0.f;
+    for (int k = 0; k < OUT; ++k) {
+      const float e = valid ? o[k] - y[(size_t)s * OUT + k] : 0.f;
+      l += e * e;
+      s_d3[t][k] = e * scale;
+    }
+    if (valid) atomicAdd(loss, l / ((float)n * (float)OUT));
+    for (int j = 0; j < H; ++j) {
+      s_h1[t][j] = valid ? h1[j] : 0.f;
+      s_h2[t][j] = valid ? h2[j] : 0.f;
+    }
+    // delta2 = (W3^T delta3) * gelu'(z2)
+    for (int j = 0; j < H; ++j) {
+      float acc = 0.f;
+      for (int k = 0; k < OUT; ++k) acc = fmaf(__ldg(params + G::W3 + k * H + j), s_d3[t][k], acc);
+      float g2;
+      gelu_f(z2[j], &g2);
+      s_d2[t][j] = valid ? acc * g2 : 0.f;
+    }
+    // delta1 = (W2^T delta2) * gelu'(z1)
+    for (int i = 0; i < H; ++i) {
+      float acc = 0.f;
+      for (int j = 0; j < H; ++j) acc = fmaf(__ldg(params + G::W2 + j * H + i), s_d2[t][j], acc);
+      float g1;
+      gelu_f(z1[i], &g1);
+      s_d1[t][i] = valid ? acc * g1 : 0.f;
+    }
+  }
+  __syncwarp();
+  // dW3[k][j] = sum_q d3[q][k] h2[q][j]; db3[k] = sum_q d3[q][k]
+  for (int e = t; e < OUT * H; e += kBlock) {
+    const int k = e / H, j = e % H;
+    float acc = 0.f;
+    for (int q = 0; q < kBlock; ++q) acc = fmaf(s_d3[q][k], s_h2[q][j], acc);
+    atomicAdd(grad + G::W3 + e, acc);
+  }
+  for (int k = t; k < OUT; k += kBlock) {
+    float acc = 0.f;
+    for (int q = 0; q < kBlock; ++q) acc += s_d3[q][k];
+    atomicAdd(grad + G::B3 + k, acc);
+  }
+  // dW2[j][i] = sum_q d2[q][j] h1[q][i]; db2, db1
+  for (int e = t; e < H * H; e += kBlock) {
+    const int j = e / H, i = e % H;
+    float acc = 0.f;
+    for (int q = 0; q < kBlock; ++q) acc = fmaf(s_d2[q][j], s_h1[q][i], acc);
+    atomicAdd(grad + G::W2 + e, acc);
+  }
+  for (int j = t; j < H; j += kBlock) {
+    float a2 = 0.f, a1 = 0.f;
+    for (int q = 0; q < kBlock; ++q) { a2 += s_d2[q][j]; a1 += s_d1[q][j]; }
+    atomicAdd(grad + G::B2 + j, a2);
+    atomicAdd(grad + G::B1 + j, a1);
+  }
+  // dW1[j][i] = sum_q d1[q][j] x[q][i]
+  for (int e = t; e < H * IN; e += kBlock) {
+    const int j = e / IN, i = e % IN;
+    float acc = 0.f;
+    for (int q = 0; q < kBlock; ++q) acc = fmaf(s_d1[q][j], s_x[q][i], acc);
+    atomicAdd(grad + G::W1 + e, acc);
+  }
+}
+
+}  // namespace wmlp
 }  // namespace soi

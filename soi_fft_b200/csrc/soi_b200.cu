@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <math.h>
+#include <cmath>
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -89,6 +90,9 @@ struct Plan {
   // tensor-core stage 1 (split form, n = 5, d = 4, S in {32, 64, 128}, B <= 72 taps)
   int s1_tc = 0;
   void *d_btc = nullptr;            // [S][16 rows][72 taps] TF32 hi/lo filter, the MMA's B layout
+  // a caller's window (soi_init_window_status): y(t) at the taps, [B][n][S],
+  // and its transform at xi = j/M - 1/2, j <= M/2; empty: the analytic window
+  std::vector<double> cw_time, cw_freq;
   bool timing = false;
   cudaEvent_t ev[5] = {};
   float ms[4] = {0, 0, 0, 0};
@@ -169,10 +173,13 @@ long double window_y(long double t, double tau, double sigma)
   return sinl(a) / a * expl(-kPi * kPi * t * t / (long double)sigma);
 }
 
+// With ytime / yfreq (a caller's window, soi_init_window_status) the real
+// window y(t) at the taps and its Fourier transform at xi = j/M - 1/2,
+// j <= M/2, replace the analytic y and y_W.
 void host_tables(size_t N, size_t S, int n, int d, size_t B, double tau, double sigma, int atap,
                  std::vector<long double> *filt, std::vector<long double> *ph_re,
                  std::vector<long double> *ph_im, std::vector<long double> *wi_re,
-                 std::vector<long double> *wi_im)
+                 std::vector<long double> *wi_im, const double *ytime = nullptr, const double *yfreq = nullptr)
 {
   const long long kappa = (long long)B - d;
   const long double mu = (long double)n / d;
@@ -186,7 +193,7 @@ void host_tables(size_t N, size_t S, int n, int d, size_t B, double tau, double 
           long long num = 2LL * th * d * (long long)S - 2LL * (long long)kk * n * (long long)S -
                           2LL * (long long)s * n + kappa * n * (long long)S;
           long double t = (long double)num / (long double)den;
-          long double y = window_y(t, tau, sigma) / mu;
+          long double y = (ytime ? (long double)ytime[(kk * n + th) * S + s] : window_y(t, tau, sigma)) / mu;
           (*filt)[(kk * n + th) * S + s] = (kk & 1) ? -y : y;
         }
   }
@@ -212,7 +219,8 @@ void host_tables(size_t N, size_t S, int n, int d, size_t B, double tau, double 
     const long double sq = sqrtl((long double)sigma);
     for (size_t i = 0; i < M; ++i) {
       long double t = (long double)i / (long double)M - 0.5L;
-      long double y = (erfcl(sq * (t - tau / 2.0L)) - erfcl(sq * (t + tau / 2.0L))) / (2.0L * tau);
+      long double y = yfreq ? (long double)yfreq[std::min(i, M - i)]
+                            : (erfcl(sq * (t - tau / 2.0L)) - erfcl(sq * (t + tau / 2.0L))) / (2.0L * tau);
       long long q = (long long)(((unsigned long long)kappa * i) % (2ULL * M));
       long double ang = -kPi * (long double)q / (long double)M;
       (*wi_re)[i] = cosl(ang) / y;
@@ -427,7 +435,8 @@ int build_ct_tables(Plan &p, const S2ChoiceCT &c)
   std::vector<R> af(half);
   for (size_t i = 0; i < half; ++i) {
     long double t = (long double)i / (long double)M - 0.5L;
-    long double y = (erfcl(sq * (t - p.tau / 2.0L)) - erfcl(sq * (t + p.tau / 2.0L))) / (2.0L * p.tau);
+    long double y = !p.cw_freq.empty() ? (long double)p.cw_freq[i]
+                                       : (erfcl(sq * (t - p.tau / 2.0L)) - erfcl(sq * (t + p.tau / 2.0L))) / (2.0L * p.tau);
     af[i] = (R)(1.0L / y);
   }
   const long long M1 = c.M1, M2 = c.M2, C = c.C;
@@ -854,7 +863,8 @@ template <typename R>
 int build_tables(Plan &p)
 {
   std::vector<long double> filt, phr, phi, wir, wii;
-  host_tables(p.N, p.S, p.nmu, p.dmu, p.B, p.tau, p.sigma, p.atap, &filt, &phr, &phi, &wir, &wii);
+  host_tables(p.N, p.S, p.nmu, p.dmu, p.B, p.tau, p.sigma, p.atap, &filt, &phr, &phi, &wir, &wii,
+              p.cw_time.empty() ? nullptr : p.cw_time.data(), p.cw_freq.empty() ? nullptr : p.cw_freq.data());
   std::vector<R> f(filt.size());
   for (size_t i = 0; i < filt.size(); ++i) f[i] = (R)filt[i];
   std::vector<R> ph, wi;
@@ -1012,13 +1022,20 @@ void make_pass1_map(Plan &p)
   p.tma1 = r == CUDA_SUCCESS;
 }
 
-int make_plan(const soi_desc_t *d, size_t k, int knob_s1_nt, int knob_s2, bool with_stream, Plan **out)
+int make_plan(const soi_desc_t *d, size_t k, int knob_s1_nt, int knob_s2, bool with_stream, Plan **out,
+              const double *y_time = nullptr, const double *y_freq = nullptr)
 {
   Plan *p = new Plan();
   p->knob_s1_nt = knob_s1_nt;
   p->knob_s2 = knob_s2;
   int rc = plan_geometry(d, k, *p);
   if (rc) { delete p; return rc; }
+  if (y_time && y_freq) {
+    p->cw_time.assign(y_time, y_time + p->B * (size_t)p->nmu * p->S);
+    p->cw_freq.assign(y_freq, y_freq + p->M / 2 + 1);
+    for (double v : p->cw_freq)
+      if (!(v > 0) || !std::isfinite(v)) { delete p; return SOI_ERR_INVALID; }   // 1/y_W must exist
+  }
   cudaError_t ce = cudaSetDevice(d->device);
   if (ce != cudaSuccess) { delete p; return SOI_ERR_CUDA; }
   rc = p->prec == SOI_PRECISION_FP64 ? build_tables<double>(*p) : build_tables<float>(*p);
@@ -1057,10 +1074,10 @@ int make_plan(const soi_desc_t *d, size_t k, int knob_s1_nt, int knob_s2, bool w
   return SOI_OK;
 }
 
-int init_plan(soi_desc_t *d, size_t k)
+int init_plan(soi_desc_t *d, size_t k, const double *y_time = nullptr, const double *y_freq = nullptr)
 {
   Plan *p = nullptr;
-  int rc = make_plan(d, k, -1, -1, true, &p);
+  int rc = make_plan(d, k, -1, -1, true, &p, y_time, y_freq);
   if (rc) return rc;
   d->plan = p;
   return SOI_OK;
@@ -1480,6 +1497,24 @@ int soi_init_status(soi_desc_t *d, soi_comm_t comm, cfft_size_t k)
   return rc;
 }
 
+int soi_init_window_status(soi_desc_t *d, soi_comm_t comm, cfft_size_t k, const double *y_time, const double *y_freq)
+{
+  if (!y_time || !y_freq) return SOI_ERR_INVALID;
+  if (!d) return SOI_ERR_INVALID;
+  d->comm = comm;
+  d->k = k;
+  if (d->plan) { free_plan((Plan *)d->plan); d->plan = nullptr; }
+  int rc = init_plan(d, k, y_time, y_freq);
+  if (rc == SOI_OK) {
+    free(d->segmentBoundaries);
+    d->segmentBoundaries = (int *)malloc(sizeof(int) * 2);   // pfft.c:144-147 with P = 1
+    d->segmentBoundaries[0] = 0;
+    d->segmentBoundaries[1] = (int)k;
+  }
+  d->last_status = rc;
+  return rc;
+}
+
 void init_soi_descriptor(soi_desc_t *d, soi_comm_t comm, cfft_size_t k)
 {
   die_on(soi_init_status(d, comm, k), "init_soi_descriptor");
@@ -1751,6 +1786,41 @@ int soi_window_tables(cfft_size_t N, cfft_size_t S, int n_mu, int d_mu, cfft_siz
 }
 
 int soi_mlp_param_count(void) { return kMlpParams; }
+
+int soi_wmlp_param_count(void) { return wmlp::kParams; }
+
+int soi_wmlp_forward_device(const float *params, const float *x, float *y, int n, void *stream)
+{
+  if (!params || !x || !y || n <= 0) return SOI_ERR_INVALID;
+  const int blocks = std::min(1024, (n + 63) / 64);
+  wmlp::forward_kernel<wmlp::kIn, wmlp::kOut><<<blocks, 64, 0, (cudaStream_t)stream>>>(params, x, y, n);
+  CK(cudaGetLastError());
+  return SOI_OK;
+}
+
+int soi_wmlp_grad_device(const float *params, const float *x, const float *y, int n, float *grad, float *loss,
+                         void *stream)
+{
+  if (!params || !x || !y || !grad || !loss || n <= 0) return SOI_ERR_INVALID;
+  cudaStream_t st = (cudaStream_t)stream;
+  CK(cudaMemsetAsync(grad, 0, wmlp::kParams * sizeof(float), st));
+  CK(cudaMemsetAsync(loss, 0, sizeof(float), st));
+  wmlp::grad_kernel<wmlp::kIn, wmlp::kOut><<<(n + wmlp::kBlock - 1) / wmlp::kBlock, wmlp::kBlock, 0, st>>>(
+      params, x, y, n, grad, loss);
+  CK(cudaGetLastError());
+  return SOI_OK;
+}
+
+int soi_adam_device(float *params, float *m, float *v, const float *grad, int count, float lr, int step,
+                    void *stream)
+{
+  if (!params || !m || !v || !grad || count <= 0 || step < 1) return SOI_ERR_INVALID;
+  mlp_adam_kernel<<<std::min(1024, (count + 255) / 256), 256, 0, (cudaStream_t)stream>>>(params, m, v, grad, count,
+                                                                                         lr, 0.9f, 0.999f, 1e-8f,
+                                                                                         step);
+  CK(cudaGetLastError());
+  return SOI_OK;
+}
 
 int soi_mlp_forward_device(const float *params, const float *x, float *y, int n, void *stream)
 {

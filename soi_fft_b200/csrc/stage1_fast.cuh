@@ -304,7 +304,12 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_conv_sfft_tS(Conv2Args a)
     long long it = 0;
     while (!mbar_try_wait(&s_mbar[p & 1], (unsigned)((p >> 1) & 1))) {
       if (++it > kBulkWaitLimit) {
+        // late copies: flag them, then wait for them to land (bounded, 16x
+        // longer) so that none is still writing shared memory when the
+        // buffer is refilled or the CTA leaves
         if (tid == 0) atomicExch(a.err, 1);
+        long long drain = 0;
+        while (!mbar_try_wait(&s_mbar[p & 1], (unsigned)((p >> 1) & 1)) && ++drain <= 16 * kBulkWaitLimit) {}
         break;
       }
     }

@@ -341,7 +341,14 @@ __global__ void __launch_bounds__(NT, MINB) k_stage2_ct(S2ArgsCT a, const __grid
         long long it = 0;
         while (!mbar_try_wait(&s_bar, bphase)) {
           if (++it > kBulkWaitLimit) {
-            if (tid == 0) atomicExch(a.err, 1);             // no further tasks are taken
+            // the copy is late: flag it (no further tasks are taken), then
+            // wait for it to land (bounded, 16x longer), so that no copy is
+            // still writing this CTA's shared memory when the tile buffer is
+            // reused or the CTA leaves; the tile computed from it is discarded
+            // with the transform (SOI_ERR_TIMEOUT)
+            if (tid == 0) atomicExch(a.err, 1);
+            long long drain = 0;
+            while (!mbar_try_wait(&s_bar, bphase) && ++drain <= 16 * kBulkWaitLimit) {}
             break;
           }
         }

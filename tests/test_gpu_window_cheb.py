@@ -88,10 +88,10 @@ def test_proposer_gradient_matches_the_cpu_network():
 def test_proposer_training_reduces_the_loss():
     rng = np.random.default_rng(1)
     x = rng.uniform(-1, 1, (512, 2)).astype(np.float32)
-    y = np.stack([np.sin(x[:, 0] * (k + 1)) + x[:, 1] * k / 32 for k in range(32)], 1).astype(np.float32)
+    y = np.stack([np.sin(x[:, 0] * (1 + k / 16)) + 0.5 * x[:, 1] * np.cos(k) for k in range(32)], 1)
     net = wc.WindowProposer(seed=2)
-    hist = net.train(x, y, steps=600, lr=3e-3)
-    assert hist[-1] < 0.2 * hist[0]
+    hist = net.train(x, y.astype(np.float32), steps=1500, lr=3e-3)
+    assert hist[-1] < 0.1 * hist[0]
 
 
 @pytest.mark.skipif(not os.path.exists(wc.WEIGHTS), reason="the trained proposer is not in the package")

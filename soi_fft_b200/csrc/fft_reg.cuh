@@ -300,4 +300,77 @@ __device__ __forceinline__ void tile_fft_ct_dense(V *sm, const V *__restrict__ t
   }
 }
 
+// The tile FFT on C dense rows of L elements at row pitch PR, as bulk copies
+// lay whole rows out: element (col, pos) at col*PR + pos, no pad inside a row.
+// With 8-byte elements and PR = 4 (mod 16), a half-warp of the first and
+// middle stages (4 columns x 4 consecutive butterflies) falls on distinct
+// banks; the last stage's half-warp (4 columns x 4 butterflies RL positions
+// apart) reads its positions in the order r ^ (blk & 3), which keeps it on
+// distinct banks too, and two conditional swaps restore the order.  Same
+// stages, twiddles and epilogue as tile_fft_ct.
+template <typename V, int R0, int R1, int R2, int C, int PR, int NT, class Emit>
+__device__ __forceinline__ void tile_fft_rows(V *sm, const V *__restrict__ tw, const Emit &emit)
+{
+  constexpr int RL = (R2 > 1) ? R2 : R1;
+  constexpr int L = R0 * R1 * R2;
+  constexpr int span0 = L / R0;
+  static_assert(RL % 4 == 0, "the last stage's read order needs RL a multiple of 4");
+  {
+    constexpr int n = C * span0;
+#pragma unroll 1
+    for (int q = threadIdx.x; q < n; q += NT) {
+      const int col = q % C, i = q / C;
+      V *p = sm + col * PR + i;
+      V v[R0];
+#pragma unroll
+      for (int r = 0; r < R0; ++r) v[r] = p[r * span0];
+      RegDFT<V, R0>::run(v);
+      p[0] = v[0];
+#pragma unroll
+      for (int k = 1; k < R0; ++k) p[k * span0] = cmul(v[k], __ldg(tw + (k - 1) * span0 + i));
+    }
+  }
+  __syncthreads();
+  if constexpr (R2 > 1) {
+    constexpr int span1 = span0 / R1;                       // = RL
+    constexpr int n = C * (L / R1);
+#pragma unroll 1
+    for (int q = threadIdx.x; q < n; q += NT) {
+      const int col = q % C, t = q / C;
+      const int blk = t / span1, i = t - blk * span1;
+      V *p = sm + col * PR + blk * span0 + i;
+      V v[R1];
+#pragma unroll
+      for (int r = 0; r < R1; ++r) v[r] = p[r * RL];
+      RegDFT<V, R1>::run(v);
+      p[0] = v[0];
+#pragma unroll
+      for (int k = 1; k < R1; ++k) p[k * RL] = cmul(v[k], __ldg(tw + (R0 - 1) * span0 + (k - 1) * span1 + i));
+    }
+    __syncthreads();
+  }
+  {
+    constexpr int n = C * (L / RL);
+#pragma unroll 1
+    for (int q = threadIdx.x; q < n; q += NT) {
+      const int col = q % C, blk = q / C;
+      const V *p = sm + col * PR + blk * RL;
+      int fbase;
+      if constexpr (R2 > 1) fbase = (blk / R1) + R0 * (blk % R1);
+      else fbase = blk;
+      const auto pre = emit.prepare(col, fbase, blk);
+      const int x = blk & 3;
+      V u[RL], v[RL];
+#pragma unroll
+      for (int r = 0; r < RL; ++r) u[r] = p[r ^ x];
+#pragma unroll
+      for (int r = 0; r < RL; ++r) v[r] = (x & 1) ? u[r ^ 1] : u[r];
+#pragma unroll
+      for (int r = 0; r < RL; ++r) u[r] = (x & 2) ? v[r ^ 2] : v[r];
+      RegDFT<V, RL>::run(u);
+      emit.template run<RL>(col, fbase, L / RL, u, pre, blk);
+    }
+  }
+}
+
 }  // namespace soi

@@ -7,6 +7,11 @@
 // in place.  Pass 2 (tile = C rows k1): FFT of length M2 of row k1, output
 // k = k1 + M1*k2, times W_inv[k], stored for k < M (the discard).
 //
+// Pass-1 tiles (M1 rows of one 32-byte run each) arrive by 2-D tensor copies;
+// pass-2 tiles (C whole rows of M2 contiguous elements) by C bulk copies into
+// rows at a bank-skewed pitch (FP32 instances; cp.async into a padded tile
+// otherwise), both off the load/store path.
+//
 // Each tile FFT is an in-place decimation-in-frequency transform with "fat"
 // radices held in registers (RegDFT), two or three radix stages with one pass
 // through shared memory between stages; the last stage stores straight to
@@ -102,6 +107,7 @@ struct S2ArgsCT {
   int wait_extra;             // 0; a test sets 1 to make every pass-2 wait run out
   int tail;                   // pass-2 tasks that end a block after its interleaved part (0 .. M1/C)
   int amp_keep;               // 1: amp loads carry an L2 evict_last hint
+  int bulk2;                  // 1: pass-2 rows arrive by bulk copies (FP32 instances)
   unsigned int *counter, *done1;
   int *err;
 };
@@ -223,6 +229,9 @@ struct S2Geom {
   // or 8 sixteen-byte slots): pitch = (slots / C) mod slots
   static constexpr int SLOTS = 128 / E;
   static constexpr int PS2 = round_up_to_residue<M2 + M2 / RLB, SLOTS, (SLOTS / C) % SLOTS>();
+  // pass-2 rows by bulk copies: whole rows at pitch PR2 = 4 (mod 16) elements
+  static constexpr int PR2 = M2 + 4;
+  static constexpr bool BULK2 = E == 8 && C == 4 && RLB % 4 == 0 && M2 % 16 == 0;
   // pass-1 tensor copies: boxes of BOXR rows (the largest divisor of M1 of at
   // most 256 rows that is a multiple of 32 rows, so every box starts 1024-byte
   // aligned), into a dense tile aligned to 1024 bytes inside the buffer
@@ -378,6 +387,42 @@ __global__ void __launch_bounds__(NT, MINB) k_stage2_ct(S2ArgsCT a, const __grid
         atomicAdd(a.done1 + seg, 1u);                         // publish, then take the next task
         take(slot ^ 1);
       }
+    } else if (G::BULK2 && a.bulk2) {
+      // C whole rows k1 (C*M2 contiguous elements) by C bulk copies into rows
+      // at pitch PR2, onto the same mbarrier as pass 1's tensor copies
+      const int k1_0 = tile * C;
+      const V *src = Tseg + k1_0 * M2;
+      static_assert(!G::BULK2 || C * G::PR2 <= G::BUF, "pass-2 rows fit the tile buffer");
+      if (tid == 0) {
+        fence_proxy_async_smem();                           // the previous task's accesses of the buffer come first
+        mbar_expect_tx(&s_bar, (unsigned int)(C * M2 * G::E));
+#pragma unroll
+        for (int c = 0; c < C; ++c) bulk_g2s(buf + c * G::PR2, src + c * M2, (unsigned)(M2 * G::E), &s_bar);
+      }
+      if (tid < C) s_tab[tid] = two_level<V>(a.dlo, a.dhi, a.dlo_bits, k1_0 + tid);
+      long long it = 0;
+      while (!mbar_try_wait(&s_bar, bphase)) {
+        if (++it > kBulkWaitLimit) {
+          // late copies: flag them (no further tasks are taken), then wait for
+          // them to land (bounded, 16x longer) before the buffer is reused or
+          // the CTA leaves
+          if (tid == 0) atomicExch(a.err, 1);
+          long long drain = 0;
+          while (!mbar_try_wait(&s_bar, bphase) && ++drain <= 16 * kBulkWaitLimit) {}
+          break;
+        }
+      }
+      bphase ^= 1u;
+      __syncthreads();
+      if (a.discard) {
+        const char *base = reinterpret_cast<const char *>(src);
+        constexpr int nlines = C * M2 * G::E / 128;
+        for (int l = tid; l < nlines; l += NT) discard_l2_line(base + l * 128);
+      }
+      EmitRowsCT<V, M1, M2, C, RLB, (MINB <= 2)> e{ reinterpret_cast<V *>(a.out) + (size_t)(a.seg_lo + seg) * a.M, k1_0, s_tab, &a,
+                                                    amp_pol };
+      if constexpr (G::BULK2) tile_fft_rows<V, B0, B1, B2, C, G::PR2, NT>(buf, reinterpret_cast<const V *>(a.tw2), e);
+      if (tid == 0) take(slot ^ 1);                           // after thread 0's own stores
     } else {
       const int k1_0 = tile * C;
       const V *src = Tseg + k1_0 * M2;

@@ -286,3 +286,26 @@ def test_stage2_schedule_does_not_change_results(N, S, prec, band, monkeypatch):
         finally:
             d.free()
     assert torch.equal(outs[0], outs[2]) and torch.equal(outs[1], outs[2])
+
+
+@pytest.mark.parametrize("N,S", [(1 << 20, 16), (1 << 22, 32), (1 << 27, 32)])
+@pytest.mark.parametrize("band", ["all", (3, 7)])
+def test_bulk_copied_pass2_rows_equal_cp_async_rows(N, S, band, monkeypatch):
+    # pass-2 rows by bulk copies (dense rows, the last radix reading in an XOR
+    # order) or by cp.async (a padded tile): the same arithmetic on the same
+    # values, so the outputs are identical
+    prec = sb.PRECISION_SPLIT_FP32
+    x = _input(N, prec)
+    lo, hi = (0, S) if band == "all" else band
+    outs = []
+    for bulk in ("1", "0"):
+        monkeypatch.setenv("SOI_STAGE2_BULK2", bulk)
+        d = _desc(N, S, prec)
+        try:
+            y = torch.zeros_like(x)
+            d.compute_segments(x, y, lo, hi)
+            torch.cuda.synchronize()
+            outs.append(y)
+        finally:
+            d.free()
+    assert torch.equal(outs[0], outs[1])

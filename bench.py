@@ -227,6 +227,24 @@ class ClockSampler:
                 "samples": len(sm), "sm_mhz_min": min(sm), "source": src}
 
 
+def gpu_local_cpus(index):
+    """The host CPUs NVML lists as local to GPU `index` (its NUMA node), or
+    None.  Read-only query."""
+    try:
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        pr = torch.cuda.get_device_properties(index)
+        bus = "%08x:%02x:%02x.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+        h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        words = pynvml.nvmlDeviceGetCpuAffinity(h, (os.cpu_count() + 63) // 64)
+        cpus = {64 * w + b for w, m in enumerate(words) for b in range(64) if (m >> b) & 1}
+        cpus &= os.sched_getaffinity(0)
+        return cpus or None
+    except Exception:
+        return None
+
+
 def dist_setup(args):
     """One process per GPU (torchrun's RANK/LOCAL_RANK/WORLD_SIZE); NCCL for
     the barrier and the max-over-ranks time, gloo where there is no GPU."""
@@ -448,6 +466,13 @@ def run_ours(args):
     # uploads its input and downloads its result.  The streamed call overlaps
     # one step's upload with the previous step's kernels and download; the
     # one-at-a-time call (compute_soi's form) is reported beside it.
+    # pinned buffers on the GPU's own NUMA node (allocated and first touched
+    # from its local CPUs, as a deployment pins its host threads), the
+    # previous affinity restored after the e2e runs
+    old_aff = os.sched_getaffinity(0)
+    local_cpus = gpu_local_cpus(local)
+    if local_cpus:
+        os.sched_setaffinity(0, local_cpus)
     h_in = torch.empty(N, dtype=x32.dtype, pin_memory=True)
     h_in.copy_(x32)
     h_out = torch.empty(N, dtype=x32.dtype, pin_memory=True)
@@ -470,8 +495,28 @@ def run_ours(args):
     e1.record(stream)
     barrier()
     single_ms = max_over_ranks_(e0.elapsed_time(e1) / 2)
+    # the host link's own time for one step's bytes: the same upload and
+    # download at once on two streams, no kernels (the streamed call's floor)
+    s_up, s_dn = torch.cuda.Stream(local), torch.cuda.Stream(local)
+    d_tmp = torch.empty_like(x32)
+    link = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        e0.record(s_up)
+        s_dn.wait_event(e0)
+        with torch.cuda.stream(s_up):
+            d_tmp.copy_(h_in, non_blocking=True)
+        with torch.cuda.stream(s_dn):
+            h_out.copy_(y32, non_blocking=True)
+        s_up.wait_stream(s_dn)
+        e1.record(s_up)
+        e1.synchronize()
+        link.append(e0.elapsed_time(e1))
+    link_ms = max_over_ranks_(min(link))
+    del d_tmp
     d32.free()
     del h_in, h_out
+    os.sched_setaffinity(0, old_aff)
 
     # ---- plain FP64 method at the same N
     fp64 = None
@@ -574,6 +619,10 @@ def run_ours(args):
                         "h2d_bytes_per_step": N * ELEM, "d2h_bytes_per_step": N * ELEM,
                         "api": "soi_compute_stream_status, %d transforms per call, pinned host buffers" % e2e_steps,
                         "matches_device_result": e2e_matches,
+                        "host_link_ms": link_ms,
+                        "host_link_note": "one step's upload and download at once on two streams, no kernels: "
+                                          "the streamed call's floor",
+                        "host_cpus": "%d NUMA-local to the GPU" % len(local_cpus) if local_cpus else "unpinned",
                         "one_at_a_time": {"api": "soi_compute_oop_status", "ms_per_step": single_ms,
                                           "value": world * flop(N) / (single_ms / 1e3) / 1e9}},
                 "gpu_launches": launches_per_step * args.steps,

@@ -159,7 +159,7 @@ int soi_compute_inverse_status(soi_desc_t *desc, const void *in, void *out);
  * transform of ins[i], i < count.  Uploads, kernels and downloads of
  * neighbouring transforms overlap on separate streams (PCIe carries both
  * directions at once), so with pinned buffers the cost per transform
- * approaches one copy time instead of two plus the kernels.  Two N-element
+ * approaches one copy time instead of two plus the kernels.  Three N-element
  * device staging buffers, allocated on first use.  Returns after the last
  * download.  No counterpart in the reference. */
 int soi_compute_stream_status(soi_desc_t *desc, const void *const *ins, void *const *outs, int count);

@@ -49,6 +49,17 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, i
                : "memory");
 }
 
+// global -> shared, one box of a 3-D tiled tensor map at element coordinates
+// (x, y, z) (same rules as tma_load_2d), completing on `bar`.  No multicast.
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z,
+                                            unsigned long long *bar)
+{
+  asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+               ::"r"(smem_u32(dst)), "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z),
+               "r"(smem_u32(bar))
+               : "memory");
+}
+
 constexpr long long kBulkWaitLimit = 1ll << 22;
 
 }  // namespace soi

@@ -49,9 +49,10 @@ struct Plan {
   double2 *d_xlo = nullptr, *d_xhi = nullptr;
   void *d_T = nullptr;         // S*Mh complex
   void *d_io = nullptr;        // N complex staging for host pointers
-  void *d_io2 = nullptr;       // second staging buffer (streamed host transforms)
+  void *d_io2 = nullptr;       // second and third staging buffers (streamed host transforms)
+  void *d_io3 = nullptr;
   cudaStream_t st_in = nullptr, st_out = nullptr;   // copy streams (streamed host transforms)
-  cudaEvent_t sev[6] = {};     // in-copied[2], computed[2], out-copied[2]
+  cudaEvent_t sev[9] = {};     // in-copied[3], computed[3], out-copied[3]
   // VLC
   int *d_vlc_words = nullptr, *d_vlc_n = nullptr, *d_vlc_emax = nullptr;
   long vlc_stride = 0;
@@ -607,6 +608,29 @@ int staged_jr(int prec, int nmu)
   return nmu == 5 ? 4 : nmu == 3 ? 4 : (nmu == 8 || nmu == 9) ? 2 : 0;
 }
 
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
+
+// The stage-1 input as a 3-D tensor [J][d][S values] of 8-byte elements
+// (a split complex is one element, an FP64 complex two), with boxes of
+// JT + AC - 1 rows of one branch: one phase's rows x_b[j0 + a_lo + t] =
+// alpha row d*(j0 + a_lo + t) + b.  False when the encoder refuses (the
+// input's address or the sizes break the tensor-copy rules); the kernel then
+// copies row by row.
+bool input_rows_map(const Plan &p, const void *in, CUtensorMap *map)
+{
+  const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  const size_t e8 = p.elem / 8;
+  const size_t nr = (size_t)p.JT2 + p.AC - 1;
+  if (!enc || !in || p.S * e8 > 256 || nr > 256 || p.J > (size_t)INT32_MAX) return false;
+  const cuuint64_t dims[3] = { (cuuint64_t)(p.S * e8), (cuuint64_t)p.dmu, (cuuint64_t)p.J };
+  const cuuint64_t strides[2] = { (cuuint64_t)(p.S * p.elem), (cuuint64_t)(p.dmu * p.S * p.elem) };
+  const cuuint32_t box[3] = { (cuuint32_t)(p.S * e8), 1, (cuuint32_t)nr };
+  const cuuint32_t estr[3] = { 1, 1, 1 };
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, const_cast<void *>(in), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <typename R, int NMU, int JR, int R0, int R1, int NT, bool BULK>
 int launch_conv_tS(Plan &p, const Exec &ex)
 {
@@ -617,10 +641,13 @@ int launch_conv_tS(Plan &p, const Exec &ex)
   a.S = (int)p.S; a.d = p.dmu; a.atap = p.atap; a.JT = p.JT2; a.pitch = p.pitch; a.AC = p.AC;
   a.buf_elems = p.buf_elems;
   a.err = (int *)ex.sync;
+  CUtensorMap rmap;
+  memset(&rmap, 0, sizeof rmap);
+  if (BULK) a.tma_rows = input_rows_map(p, ex.in, &rmap) ? 1 : 0;
   auto kern = k_conv_sfft_tS<R, NMU, JR, R0, R1, NT, BULK>;
   CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem1b));
   dim3 grid((unsigned)((p.J + p.JT2 - 1) / p.JT2));
-  kern<<<grid, NT, p.smem1b, ex.st>>>(a);
+  kern<<<grid, NT, p.smem1b, ex.st>>>(a, rmap);
   CK(cudaGetLastError());
   return SOI_OK;
 }
@@ -643,7 +670,8 @@ int launch_tS_switch_nt(Plan &p, const Exec &ex)
 template <typename R, int JR>
 int launch_tS_switch(Plan &p, const Exec &ex)
 {
-  if (p.s1_nt == 256) return launch_tS_switch_nt<R, JR, 256, false>(p, ex);
+  if (p.s1_nt == 256)
+    return p.s1_bulk ? launch_tS_switch_nt<R, JR, 256, true>(p, ex) : launch_tS_switch_nt<R, JR, 256, false>(p, ex);
   return p.s1_bulk ? launch_tS_switch_nt<R, JR, 512, true>(p, ex) : launch_tS_switch_nt<R, JR, 512, false>(p, ex);
 }
 
@@ -688,14 +716,25 @@ void plan_stage1_staged(Plan &p)
   if (!jr || p.S > 512 || (p.S * p.nmu) % 4) return;
   const bool ts = tS_available(p);
   // compile-time-S kernel: 512 threads and 200 KB (one CTA per SM), or 256
-  // threads and <= 110 KB (two CTAs per SM, smaller tiles: more halo rows per
-  // output) where two thread rows fit.  512 measured faster at N = 2^29,
-  // S = 128 (6.64 vs 7.25 ms); the batch tuner tries both.
+  // threads and <= 110 KB (two CTAs per SM: one CTA's convolution overlaps
+  // the other's S-point FFT and stores; smaller tiles, more halo rows per
+  // output) where two thread rows fit.  Staged by tensor copies (one per
+  // phase, issued by one thread onto an mbarrier) instead of every thread's
+  // 16-byte cp.async, 256 threads measured fastest (stage 1 at N = 2^29,
+  // S = 128: 5.36 ms against 5.52 at 512 threads and 5.77 / 6.09 with
+  // cp.async; split S = 64 / 32 / 16 and FP64 S = 64 / 32 likewise), except
+  // FP64 at S = 128 (6.30 ms at 512 against 6.37).  The batch tuner tries both.
+  const bool bulk = ts && (p.knob_s1_bulk >= 0 ? p.knob_s1_bulk : env_int("SOI_STAGE1_BULK", 1)) != 0;
   int nt = 512;
-  if (ts && 2 * (int)p.S <= 256)
-    nt = (p.knob_s1_nt > 0 ? p.knob_s1_nt : env_int("SOI_STAGE1_NT", 512)) == 256 ? 256 : 512;
+  if (ts && 2 * (int)p.S <= 256) {
+    const int dflt = bulk && !(p.prec == SOI_PRECISION_FP64 && p.S == 128) ? 256 : 512;
+    nt = (p.knob_s1_nt > 0 ? p.knob_s1_nt : env_int("SOI_STAGE1_NT", dflt)) == 256 ? 256 : 512;
+  }
   const int groups = nt / (int)p.S;
-  const size_t budget = (nt == 256 ? 110 * 1024 : 200 * 1024) - p.S * (p.elem + sizeof(int));
+  // tensor-copy staging: buffers on 128-byte boundaries, 128 bytes of
+  // alignment slack
+  const size_t align = bulk ? 128 : 16;
+  const size_t budget = (nt == 256 ? 110 * 1024 : 200 * 1024) - p.S * (p.elem + sizeof(int)) - (bulk ? 128 : 0);
   const size_t real = p.elem / 2;
   const size_t pitch = ts ? ((p.S + p.S / tS_r1(p.S)) | 1) : (size_t)p.pitch;
   for (int jt = groups * jr; jt >= jr; jt -= jr) {
@@ -706,17 +745,14 @@ void plan_stage1_staged(Plan &p)
       size_t be = rows + fel;
       const size_t tile = (size_t)p.nmu * jt * pitch;
       be = std::max(be, (tile + 1) / 2);
-      be = (be * p.elem + 15) / 16 * 16 / p.elem;   // both buffers start on 16-byte boundaries (cp.async 16)
+      be = (be * p.elem + align - 1) / align * align / p.elem;   // both buffers start aligned
       if (2 * be * p.elem <= budget) {
         p.JR2 = jr; p.JT2 = jt; p.AC = ac; p.buf_elems = (int)be;
-        p.smem1b = 2 * be * p.elem + p.S * (p.elem + sizeof(int));
+        p.smem1b = 2 * be * p.elem + p.S * (p.elem + sizeof(int)) + (bulk ? 128 : 0);
         p.s1fast = 1;
         p.s1_tS = ts ? 1 : 0;
         p.s1_nt = ts ? nt : 512;
-        // staging by bulk copies: correct, but measured slower at N = 2^29, S = 128
-        // (7.25 vs 6.36 ms: one warp's 42 serial row copies per phase arrive later
-        // than 512 threads' 16-byte cp.async); off unless asked for
-        p.s1_bulk = ts && nt == 512 && (p.knob_s1_bulk >= 0 ? p.knob_s1_bulk : env_int("SOI_STAGE1_BULK", 0)) ? 1 : 0;
+        p.s1_bulk = bulk ? 1 : 0;
         return;
       }
     }
@@ -929,7 +965,7 @@ void free_plan(Plan *p)
   cudaGetDevice(&cur);
   cudaSetDevice(p->device);
   void *bufs[] = { p->d_filt, p->d_phase, p->d_twS, p->d_tw1, p->d_tw2, p->d_winv, p->d_wsmall,
-                   p->d_permS, p->d_perm1, p->d_perm2, p->d_xlo, p->d_xhi, p->d_T, p->d_io, p->d_io2,
+                   p->d_permS, p->d_perm1, p->d_perm2, p->d_xlo, p->d_xhi, p->d_T, p->d_io, p->d_io2, p->d_io3,
                    p->d_vlc_words, p->d_vlc_n, p->d_vlc_emax, p->d_sync, p->d_filt2, p->d_amp, p->d_dlo, p->d_dhi, p->d_ph2, p->d_ctw1, p->d_ctw2, p->d_base1, p->d_step1, p->d_btc };
   for (void *b : bufs) if (b) cudaFree(b);
   for (auto &e : p->ev) if (e) cudaEventDestroy(e);
@@ -1567,21 +1603,26 @@ int compute_stream_impl(soi_desc_t *d, const void *const *ins, void *const *outs
   const size_t bytes = p->N * p->elem;
   if (!p->d_io) CK(cudaMalloc(&p->d_io, bytes));
   if (!p->d_io2) CK(cudaMalloc(&p->d_io2, bytes));
+  if (!p->d_io3) CK(cudaMalloc(&p->d_io3, bytes));
   if (!p->st_in) CK(cudaStreamCreateWithFlags(&p->st_in, cudaStreamNonBlocking));
   if (!p->st_out) CK(cudaStreamCreateWithFlags(&p->st_out, cudaStreamNonBlocking));
   for (auto &e : p->sev)
     if (!e) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   cudaStream_t st = p->stream;
-  void *buf[2] = { p->d_io, p->d_io2 };
-  cudaEvent_t *in_done = p->sev, *comp_done = p->sev + 2, *out_done = p->sev + 4;
+  // three buffers: the upload of transform i + 1 never waits for a download
+  // (buffer i + 1 was last downloaded as transform i - 2), so in steady state
+  // the copies in both directions run back to back and the kernels hide
+  // between them
+  void *buf[3] = { p->d_io, p->d_io2, p->d_io3 };
+  cudaEvent_t *in_done = p->sev, *comp_done = p->sev + 3, *out_done = p->sev + 6;
   CK(cudaMemsetAsync(p->d_sync, 0, sizeof(unsigned int), st));
   // the copy streams start after everything already queued on the plan's stream
   CK(cudaEventRecord(comp_done[0], st));
   CK(cudaStreamWaitEvent(p->st_in, comp_done[0], 0));
   CK(cudaStreamWaitEvent(p->st_out, comp_done[0], 0));
   for (int i = 0; i < count; ++i) {
-    const int b = i & 1;
-    if (i >= 2) CK(cudaStreamWaitEvent(p->st_in, out_done[b], 0));   // buffer b drained
+    const int b = i % 3;
+    if (i >= 3) CK(cudaStreamWaitEvent(p->st_in, out_done[b], 0));   // buffer b drained
     CK(cudaMemcpyAsync(buf[b], ins[i], bytes, cudaMemcpyHostToDevice, p->st_in));
     CK(cudaEventRecord(in_done[b], p->st_in));
     CK(cudaStreamWaitEvent(st, in_done[b], 0));
@@ -1596,7 +1637,7 @@ int compute_stream_impl(soi_desc_t *d, const void *const *ins, void *const *outs
     CK(cudaEventRecord(out_done[b], p->st_out));
   }
   // the plan's stream ends after the last download
-  CK(cudaStreamWaitEvent(st, out_done[(count - 1) & 1], 0));
+  CK(cudaStreamWaitEvent(st, out_done[(count - 1) % 3], 0));
   CK(cudaStreamSynchronize(st));
   CK(cudaStreamSynchronize(p->st_out));
   return check_stage2(*p, p->d_sync, st);

@@ -31,6 +31,7 @@ struct Conv2Args {
   int buf_elems;         // complex elements per staging buffer (rows + filter, rounded)
   int seg_lo, seg_hi;    // segments sigma stored (all: 0, S)
   int *err;              // set to 1 when a staging wait gives up (bulk copies)
+  int tma_rows = 0;      // the kernel's tensor map describes alpha (bulk staging)
 };
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
@@ -220,12 +221,18 @@ template <typename V> struct EmitTransposed {
 // output straight to HBM.  Tile layout: row r, column s at
 // r*PITCH + s + s/R1, PITCH odd.
 //
-// BULK: each phase is staged by warp 0 with one bulk copy (TMA, untiled) per
-// input row and one for the filter slice, completing on the buffer's
-// mbarrier; all threads wait on the mbarrier's phase parity (bounded: a wait
-// that gives up sets a.err).  Otherwise every thread issues 16-byte cp.async.
+// BULK: thread 0 stages each phase with one tensor copy (TMA) of the
+// phase's JT + AC - 1 input rows -- a box of [rows][1 branch][S values] of
+// the input viewed as [J][d][S] -- and one bulk copy of the filter slice,
+// both completing on the buffer's mbarrier; all threads wait on the
+// mbarrier's phase parity (bounded: a wait that gives up sets a.err and then
+// drains).  A tile whose rows wrap around the input (the ghost rows of
+// .cpp:495-515) takes its rows by one bulk copy per row from warp 0 instead.
+// The buffers start on 128-byte boundaries (the tensor copy's destination
+// rule), and the filter slice sits after JT + AC - 1 rows in every phase.
+// Otherwise every thread issues 16-byte cp.async.
 template <typename R, int NMU, int JR, int R0, int R1, int NT, bool BULK>
-__global__ void __launch_bounds__(NT, 512 / NT) k_conv_sfft_tS(Conv2Args a)
+__global__ void __launch_bounds__(NT, 512 / NT) k_conv_sfft_tS(Conv2Args a, const __grid_constant__ CUtensorMap rmap)
 {
   using V = typename cplx_of<R>::type;
   constexpr int S = R0 * R1;
@@ -233,7 +240,10 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_conv_sfft_tS(Conv2Args a)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int JT = a.JT;
   const int rows_tile = NMU * JT;
-  V *buf0 = reinterpret_cast<V *>(smem_raw);
+  // 128-byte aligned start (the host reserves the slack when BULK)
+  unsigned char *smem_base = smem_raw;
+  if (BULK) smem_base += (128u - (smem_u32(smem_raw) & 127u)) & 127u;
+  V *buf0 = reinterpret_cast<V *>(smem_base);
   V *buf1 = buf0 + a.buf_elems;
   V *tile = buf0;
   V *twS = buf0 + 2 * (size_t)a.buf_elems;
@@ -282,12 +292,26 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_conv_sfft_tS(Conv2Args a)
   };
   __shared__ unsigned long long s_mbar[2];
   // the same phase as bulk copies issued by warp 0 onto the buffer's mbarrier
+  // rows of the box: JT + AC - 1 (the phase with fewer taps uses a prefix);
+  // a tile takes the tensor copy when every phase's box ends inside [0, J)
+  const int NR = JT + a.AC - 1;
+  const bool tma_rows = a.tma_rows && j0 + (nch - 1) * a.AC + NR <= a.J;
   auto issue_bulk = [&](int p, V *dst, unsigned long long *bar) {
     if (tid >= 32) return;
     const int b = p / nch, a_lo = (p % nch) * a.AC;
     const int n_a = min(a.AC, a.atap - a_lo);
     const int nrows = JT + n_a - 1;
     const unsigned fbytes = (unsigned)(n_a * NMU * S * (int)sizeof(R));
+    const R *fsrc = filt + ((size_t)(b * a.atap + a_lo) * NMU) * S;
+    if (tma_rows) {
+      if (tid == 0) {
+        mbar_expect_tx(bar, (unsigned)(NR * ROWB) + fbytes);
+        fence_proxy_async_smem();
+        tma_load_3d(dst, &rmap, 0, b, (int)(j0 + a_lo), bar);
+        bulk_g2s(dst + (size_t)NR * S, fsrc, fbytes, bar);
+      }
+      return;
+    }
     if (tid == 0) mbar_expect_tx(bar, (unsigned)(nrows * ROWB) + fbytes);
     __syncwarp();
     fence_proxy_async_smem();
@@ -296,8 +320,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_conv_sfft_tS(Conv2Args a)
       if (r >= M) r -= M;                                    // circular (ghost rows, .cpp:495-515)
       bulk_g2s(dst + (size_t)t * S, alpha + r * S, (unsigned)ROWB, bar);
     }
-    if (tid == 31)
-      bulk_g2s(dst + (size_t)nrows * S, filt + ((size_t)(b * a.atap + a_lo) * NMU) * S, fbytes, bar);
+    if (tid == 31) bulk_g2s(dst + (size_t)NR * S, fsrc, fbytes, bar);
   };
   // phase p's data has arrived: buffer p & 1, used for the (p >> 1)-th time
   auto wait_bulk = [&](int p) {
@@ -353,7 +376,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_conv_sfft_tS(Conv2Args a)
       const int n_a = min(a.AC, a.atap - a_lo);
       const int nrows = JT + n_a - 1;
       const V *rows = cur + (size_t)(jb * JR) * S + s;        // rows[t*S] = x_b[j0 + a_lo + jb*JR + t]
-      const R *fb = reinterpret_cast<const R *>(cur + (size_t)nrows * S) + s;   // fb[(u*NMU + th)*S]
+      const R *fb = reinterpret_cast<const R *>(cur + (size_t)(BULK ? NR : nrows) * S) + s;   // fb[(u*NMU + th)*S]
       V xw[JR];
 #pragma unroll
       for (int jj = 0; jj < JR - 1; ++jj) xw[jj] = rows[jj * S];

@@ -221,12 +221,20 @@ def test_misaligned_device_input_is_rejected():
         d.free()
 
 
-@pytest.mark.parametrize("N,S,prec", [(1 << 20, 16, sb.PRECISION_SPLIT_FP32), (1 << 22, 128, sb.PRECISION_SPLIT_FP32),
-                                      (1 << 18, 8, sb.PRECISION_FP64)])
-def test_bulk_copy_staging_equals_cp_async_staging(N, S, prec, monkeypatch):
-    # the two ways of staging stage 1's input rows feed identical arithmetic
+@pytest.mark.parametrize("N,S,prec,nt", [(1 << 20, 16, sb.PRECISION_SPLIT_FP32, "512"),
+                                         (1 << 22, 128, sb.PRECISION_SPLIT_FP32, "512"),
+                                         (1 << 22, 128, sb.PRECISION_SPLIT_FP32, "256"),
+                                         (1 << 24, 256, sb.PRECISION_SPLIT_FP32, "512"),
+                                         (1 << 18, 8, sb.PRECISION_FP64, "512"),
+                                         (1 << 22, 128, sb.PRECISION_FP64, "512"),
+                                         (1 << 20, 64, sb.PRECISION_FP64, "256")])
+def test_bulk_copy_staging_equals_cp_async_staging(N, S, prec, nt, monkeypatch):
+    # the two ways of staging stage 1's input rows (per-thread cp.async, or a
+    # tensor copy per phase with row-by-row bulk copies for the tiles whose
+    # rows wrap around the input) feed identical arithmetic
     x = _input(N, prec)
     outs = []
+    monkeypatch.setenv("SOI_STAGE1_NT", nt)
     for bulk in ("0", "1"):
         monkeypatch.setenv("SOI_STAGE1_BULK", bulk)
         d = _desc(N, S, prec)

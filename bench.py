@@ -571,8 +571,11 @@ def run_ours(args):
         acc2 = float(torch.linalg.norm(y2 - X2) / torch.linalg.norm(X2))
         del X2
         kern = {}
-        for key, kname in (("stage1", "k_conv_sfft_tS<double, 5, 4, 8, 8, 512, false> (convolution + 64-point FFTs "
-                                       "+ transposed store)"),
+        var = sb.plan_variant(N2, S2, sb.PRECISION_FP64)
+        s1name = ("k_conv_sfft_tS<double, 5, 4, 8, 8, %d, %s> (convolution + 64-point FFTs + transposed store, "
+                  "staged by %s)" % (var["stage1_threads"], "true" if var["stage1_staging"] == "tensor copies"
+                                     else "false", var["stage1_staging"]))
+        for key, kname in (("stage1", s1name),
                            ("stage2", "k_stage2_ct<double, 10, 16, 16, 8, 16, 16, 256, 2, 2> (M'-point four-step "
                                       "FFT + demodulation + discard)")):
             kms = statistics.mean(t[key + "_ms"] for t in st2)

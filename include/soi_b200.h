@@ -188,6 +188,12 @@ int soi_segment_fft_demod_device(soi_desc_t *desc, void *transposed_dev, void *o
  * groups per thread JR, stage-1 shared bytes, M1, M2, C1, C2, pass-1 and
  * pass-2 shared bytes, radix stages of the S-, M1- and M2-point FFTs. */
 int soi_plan_geometry(const soi_desc_t *desc, cfft_size_t k, long long *info);
+/* The kernels a plan runs, without touching a GPU: info[0] = stage-1 kernel
+ * (0 general, 1 staged, 2 compile-time S, 3 tensor cores), info[1] = its
+ * threads per CTA, info[2] = its staging (0 cp.async, 1 one tensor copy per
+ * phase), info[3] = stage 2 (0 two kernels, 1 persistent four-step),
+ * info[4] = pass-2 rows by bulk copies (1) or cp.async (0). */
+int soi_plan_variant(const soi_desc_t *desc, cfft_size_t k, int *info);
 
 /* Kernel timings of the last compute (milliseconds, CUDA events on the
  * launching stream): [0] stage 1, [1] stage 2, [2] VLC, [3] whole compute. */

@@ -327,6 +327,22 @@ def window_tables(N, S, n_mu=5, d_mu=4, B=72, tau=928 / 1024., sigma=373.7314):
     return filt.reshape(B, n_mu, S), phase.reshape(n_mu, S), winv
 
 
+def plan_variant(N, S, precision=PRECISION_FP64, n_mu=5, d_mu=4, B=72):
+    """Host-side choice of kernels (no GPU): stage-1 kernel, its threads and
+    staging, the stage-2 form and its pass-2 staging."""
+    d = _Desc()
+    lib().set_default_soi_descriptor(ctypes.byref(d))
+    d.N, d.n_mu, d.d_mu, d.B, d.precision = N, n_mu, d_mu, B, precision
+    info = (ctypes.c_int * 5)()
+    lib().soi_plan_variant.argtypes = [ctypes.POINTER(_Desc), ctypes.c_size_t, ctypes.c_void_p]
+    _check(lib().soi_plan_variant(ctypes.byref(d), S, info), "soi_plan_variant")
+    kinds = {0: "general", 1: "staged", 2: "compile-time S", 3: "tensor cores"}
+    return {"stage1": kinds[info[0]], "stage1_threads": info[1],
+            "stage1_staging": "tensor copies" if info[2] else "cp.async",
+            "stage2": "persistent" if info[3] else "two kernels",
+            "pass2_staging": "bulk copies" if info[4] else "cp.async"}
+
+
 def plan_geometry(N, S, precision=PRECISION_FP64, n_mu=5, d_mu=4, B=72):
     """Host-side plan geometry (no GPU): dict of tile shapes and splits."""
     d = _Desc()

@@ -1793,6 +1793,22 @@ int soi_plan_geometry(const soi_desc_t *d, cfft_size_t k, long long *info)
   return SOI_OK;
 }
 
+int soi_plan_variant(const soi_desc_t *d, cfft_size_t k, int *info)
+{
+  if (!info) return SOI_ERR_INVALID;
+  Plan p;
+  int rc = plan_geometry(d, k, p);
+  if (rc) return rc;
+  info[0] = p.s1_tc ? 3 : p.s1_tS ? 2 : p.s1fast ? 1 : 0;
+  info[1] = p.s1_tc ? 512 : p.s1_tS ? p.s1_nt : (p.s1fast ? 512 : 0);
+  info[2] = p.s1_tS && p.s1_bulk ? 1 : 0;
+  info[3] = p.fast2 ? 1 : 0;
+  // the persistent kernel's pass-2 bulk rows: FP32 instances, on unless
+  // SOI_STAGE2_BULK2=0 (the switch is read when the device plan is set up)
+  info[4] = p.fast2 && p.prec == SOI_PRECISION_SPLIT_FP32 && env_int("SOI_STAGE2_BULK2", 1) ? 1 : 0;
+  return SOI_OK;
+}
+
 int soi_kernels_per_compute(soi_desc_t *d)
 {
   Plan *p = plan_of(d);

@@ -128,3 +128,20 @@ def test_noalloc_rejects_oversized_requests_before_touching_the_gpu(ln, nchunks)
     # non-null stand-in pointers: the size check comes before any device access,
     # so without a GPU the call returns SOI_ERR_INVALID, not SOI_ERR_CUDA
     assert fn(ctypes.c_void_p(256), ctypes.c_void_p(256), ln, nchunks, None) == 1
+
+
+def test_plan_variant_picks_the_measured_defaults(monkeypatch):
+    # host logic only: the kernels a plan would launch
+    v = sb.plan_variant(1 << 29, 128, sb.PRECISION_SPLIT_FP32)
+    assert v == {"stage1": "compile-time S", "stage1_threads": 256, "stage1_staging": "tensor copies",
+                 "stage2": "persistent", "pass2_staging": "bulk copies"}
+    assert sb.plan_variant(1 << 28, 64, sb.PRECISION_FP64)["stage1_threads"] == 256
+    assert sb.plan_variant(1 << 28, 128, sb.PRECISION_FP64)["stage1_threads"] == 512
+    assert sb.plan_variant(1 << 28, 64, sb.PRECISION_FP64)["pass2_staging"] == "cp.async"
+    monkeypatch.setenv("SOI_STAGE1_BULK", "0")
+    v = sb.plan_variant(1 << 29, 128, sb.PRECISION_SPLIT_FP32)
+    assert (v["stage1_staging"], v["stage1_threads"]) == ("cp.async", 512)
+    monkeypatch.setenv("SOI_STAGE1_NT", "256")
+    assert sb.plan_variant(1 << 29, 128, sb.PRECISION_SPLIT_FP32)["stage1_threads"] == 256
+    monkeypatch.setenv("SOI_STAGE2_BULK2", "0")
+    assert sb.plan_variant(1 << 29, 128, sb.PRECISION_SPLIT_FP32)["pass2_staging"] == "cp.async"

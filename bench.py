@@ -72,7 +72,7 @@ KERNELS = {
 # per-output behaviour does not depend on N; stage 2 at N = 2^26, S = 16, the
 # same M' = 2560 x 2048 tiles).
 FP64_PROFILE = {
-    "stage1": {"fp64_pipe_frac": 0.518, "traffic_ratio": 2.365 / 2.416,
+    "stage1": {"fp64_pipe_frac": 0.565, "traffic_ratio": 2.369 / 2.416,
                "profile": "ncu --set full at N=2^26, S=64, same instance"},
     "stage2": {"fp64_pipe_frac": 0.242, "traffic_ratio": 5.797 / 2.416,
                "profile": "ncu --set full at N=2^26, S=16, same M' tiles"},

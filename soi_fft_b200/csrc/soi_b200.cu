@@ -68,7 +68,7 @@ struct Plan {
   size_t f2_smem = 0;
   int discard = 1;             // drop consumed intermediate lines from L2
   int amp_keep = 0;            // demodulation amplitude loads hint L2 evict_last
-  int bulk2 = 0;               // pass-2 rows by bulk copies (FP32 instances)
+  int bulk2 = 0;               // pass-2 rows by bulk copies
   int wait_extra = 0;          // failure test: pass-2 waits for a count that never comes
   void *d_amp = nullptr;            // [M1][M2] real demodulation amplitude, pass-2 store order
   void *d_ctw1 = nullptr, *d_ctw2 = nullptr;   // tile-FFT twiddles of the two passes, warp read order
@@ -539,7 +539,8 @@ int setup_s2ct(Plan &p, int idx)
   p.discard = env_int("SOI_STAGE2_DISCARD", 1);
   p.amp_keep = env_int("SOI_STAGE2_AMP_KEEP", 0) ? 1 : 0;
   // pass-2 rows by bulk copies: 5.64 vs 5.82 ms at N = 2^29, S = 128 (split),
-  // bit-identical output; SOI_STAGE2_BULK2=0 selects cp.async
+  // 6.69 vs 7.01 ms at N = 2^28, S = 64 (FP64), bit-identical output;
+  // SOI_STAGE2_BULK2=0 selects cp.async
   p.bulk2 = env_int("SOI_STAGE2_BULK2", 1) ? 1 : 0;
   // failure-detection test only: every pass-2 task then waits for one more
   // pass-1 completion than exists, runs out its iteration limit and the
@@ -1803,9 +1804,9 @@ int soi_plan_variant(const soi_desc_t *d, cfft_size_t k, int *info)
   info[1] = p.s1_tc ? 512 : p.s1_tS ? p.s1_nt : (p.s1fast ? 512 : 0);
   info[2] = p.s1_tS && p.s1_bulk ? 1 : 0;
   info[3] = p.fast2 ? 1 : 0;
-  // the persistent kernel's pass-2 bulk rows: FP32 instances, on unless
-  // SOI_STAGE2_BULK2=0 (the switch is read when the device plan is set up)
-  info[4] = p.fast2 && p.prec == SOI_PRECISION_SPLIT_FP32 && env_int("SOI_STAGE2_BULK2", 1) ? 1 : 0;
+  // the persistent kernel's pass-2 bulk rows: on unless SOI_STAGE2_BULK2=0
+  // (the switch is read when the device plan is set up)
+  info[4] = p.fast2 && env_int("SOI_STAGE2_BULK2", 1) ? 1 : 0;
   return SOI_OK;
 }
 

@@ -107,7 +107,7 @@ struct S2ArgsCT {
   int wait_extra;             // 0; a test sets 1 to make every pass-2 wait run out
   int tail;                   // pass-2 tasks that end a block after its interleaved part (0 .. M1/C)
   int amp_keep;               // 1: amp loads carry an L2 evict_last hint
-  int bulk2;                  // 1: pass-2 rows arrive by bulk copies (FP32 instances)
+  int bulk2;                  // 1: pass-2 rows arrive by bulk copies
   unsigned int *counter, *done1;
   int *err;
 };
@@ -229,9 +229,12 @@ struct S2Geom {
   // or 8 sixteen-byte slots): pitch = (slots / C) mod slots
   static constexpr int SLOTS = 128 / E;
   static constexpr int PS2 = round_up_to_residue<M2 + M2 / RLB, SLOTS, (SLOTS / C) % SLOTS>();
-  // pass-2 rows by bulk copies: whole rows at pitch PR2 = 4 (mod 16) elements
+  // pass-2 rows by bulk copies: whole rows at pitch PR2 = 4 (mod SLOTS)
+  // elements, so the C rows of a task start SLOTS / C slots apart (FP32, C = 4:
+  // 4 of 16 eight-byte slots; FP64, C = 2: 4 of 8 sixteen-byte slots), and the
+  // last radix's XOR read order spreads a group of 4 butterflies over 4 slots
   static constexpr int PR2 = M2 + 4;
-  static constexpr bool BULK2 = E == 8 && C == 4 && RLB % 4 == 0 && M2 % 16 == 0;
+  static constexpr bool BULK2 = ((E == 8 && C == 4) || (E == 16 && C == 2)) && RLB % 4 == 0 && M2 % 16 == 0;
   // pass-1 tensor copies: boxes of BOXR rows (the largest divisor of M1 of at
   // most 256 rows that is a multiple of 32 rows, so every box starts 1024-byte
   // aligned), into a dense tile aligned to 1024 bytes inside the buffer

@@ -137,7 +137,7 @@ def test_plan_variant_picks_the_measured_defaults(monkeypatch):
                  "stage2": "persistent", "pass2_staging": "bulk copies"}
     assert sb.plan_variant(1 << 28, 64, sb.PRECISION_FP64)["stage1_threads"] == 256
     assert sb.plan_variant(1 << 28, 128, sb.PRECISION_FP64)["stage1_threads"] == 512
-    assert sb.plan_variant(1 << 28, 64, sb.PRECISION_FP64)["pass2_staging"] == "cp.async"
+    assert sb.plan_variant(1 << 28, 64, sb.PRECISION_FP64)["pass2_staging"] == "bulk copies"
     monkeypatch.setenv("SOI_STAGE1_BULK", "0")
     v = sb.plan_variant(1 << 29, 128, sb.PRECISION_SPLIT_FP32)
     assert (v["stage1_staging"], v["stage1_threads"]) == ("cp.async", 512)

@@ -296,13 +296,14 @@ def test_stage2_schedule_does_not_change_results(N, S, prec, band, monkeypatch):
     assert torch.equal(outs[0], outs[2]) and torch.equal(outs[1], outs[2])
 
 
-@pytest.mark.parametrize("N,S", [(1 << 20, 16), (1 << 22, 32), (1 << 27, 32)])
+@pytest.mark.parametrize("N,S,prec", [(1 << 20, 16, sb.PRECISION_SPLIT_FP32), (1 << 22, 32, sb.PRECISION_SPLIT_FP32),
+                                      (1 << 27, 32, sb.PRECISION_SPLIT_FP32), (1 << 20, 8, sb.PRECISION_FP64),
+                                      (1 << 22, 16, sb.PRECISION_FP64), (1 << 26, 16, sb.PRECISION_FP64)])
 @pytest.mark.parametrize("band", ["all", (3, 7)])
-def test_bulk_copied_pass2_rows_equal_cp_async_rows(N, S, band, monkeypatch):
+def test_bulk_copied_pass2_rows_equal_cp_async_rows(N, S, prec, band, monkeypatch):
     # pass-2 rows by bulk copies (dense rows, the last radix reading in an XOR
     # order) or by cp.async (a padded tile): the same arithmetic on the same
     # values, so the outputs are identical
-    prec = sb.PRECISION_SPLIT_FP32
     x = _input(N, prec)
     lo, hi = (0, S) if band == "all" else band
     outs = []

@@ -82,7 +82,7 @@ struct Plan {
   int s1fast = 0, JR2 = 0, JT2 = 0, AC = 0, buf_elems = 0;
   int s1_tS = 0;                    // compile-time-S stage-1 instance available
   int s1_nt = 512;                  // its block size (256: two CTAs per SM)
-  int s1_bulk = 0;                  // its staging by bulk copies (512 threads)
+  int s1_bulk = 0;                  // its staging by tensor copies
   size_t smem1b = 0;
   void *d_filt2 = nullptr;          // [d][atap][nmu][S] real
   // variant choices forced by the batch tuner (-1: defaults / SOI_* switches)
@@ -725,10 +725,16 @@ void plan_stage1_staged(Plan &p)
   // S = 128: 5.36 ms against 5.52 at 512 threads and 5.77 / 6.09 with
   // cp.async; split S = 64 / 32 / 16 and FP64 S = 64 / 32 likewise), except
   // FP64 at S = 128 (6.30 ms at 512 against 6.37).  The batch tuner tries both.
-  const bool bulk = ts && (p.knob_s1_bulk >= 0 ? p.knob_s1_bulk : env_int("SOI_STAGE1_BULK", 1)) != 0;
+  // A phase's rows are one tensor-copy box: at most 256 values of 8 bytes
+  // per row and 256 rows, so wider rows stay with cp.async and the tile
+  // search below keeps JT + B/d - 1 <= 256.  Rows of 64 bytes (split, S = 8)
+  // measured faster with cp.async (2^24: 0.179 vs 0.205 ms; 2^20: 0.022 vs
+  // 0.050), and 256 threads there too.
+  const bool bulk = ts && (p.knob_s1_bulk >= 0 ? p.knob_s1_bulk : env_int("SOI_STAGE1_BULK", 1)) != 0 &&
+                    p.S * (p.elem / 8) <= 256 && p.S * p.elem >= 128;
   int nt = 512;
   if (ts && 2 * (int)p.S <= 256) {
-    const int dflt = bulk && !(p.prec == SOI_PRECISION_FP64 && p.S == 128) ? 256 : 512;
+    const int dflt = p.prec == SOI_PRECISION_FP64 && p.S == 128 ? 512 : (bulk || p.S <= 64) ? 256 : 512;
     nt = (p.knob_s1_nt > 0 ? p.knob_s1_nt : env_int("SOI_STAGE1_NT", dflt)) == 256 ? 256 : 512;
   }
   const int groups = nt / (int)p.S;
@@ -740,12 +746,13 @@ void plan_stage1_staged(Plan &p)
   const size_t pitch = ts ? ((p.S + p.S / tS_r1(p.S)) | 1) : (size_t)p.pitch;
   for (int jt = groups * jr; jt >= jr; jt -= jr) {
     if ((long long)jt > (long long)p.J - p.atap - jt) continue;     // keep the wrap single-step
+    if (bulk && jt + p.atap - 1 > 256) continue;               // every tap count fits one box
     for (int ac = p.atap; ac >= 1; --ac) {
       const size_t rows = (size_t)(jt + ac - 1) * p.S;
       const size_t fel = ((size_t)ac * p.nmu * p.S * real + p.elem - 1) / p.elem;
       size_t be = rows + fel;
       const size_t tile = (size_t)p.nmu * jt * pitch;
-      be = std::max(be, (tile + 1) / 2);
+      be = std::max(be, (tile + 1) / 2);                        // the FFT tile aliases the buffers
       be = (be * p.elem + align - 1) / align * align / p.elem;   // both buffers start aligned
       if (2 * be * p.elem <= budget) {
         p.JR2 = jr; p.JT2 = jt; p.AC = ac; p.buf_elems = (int)be;

@@ -221,7 +221,9 @@ def test_misaligned_device_input_is_rejected():
         d.free()
 
 
-@pytest.mark.parametrize("N,S,prec,nt", [(1 << 20, 16, sb.PRECISION_SPLIT_FP32, "512"),
+@pytest.mark.parametrize("N,S,prec,nt", [(1 << 16, 8, sb.PRECISION_SPLIT_FP32, "512"),
+                                         (1 << 18, 8, sb.PRECISION_SPLIT_FP32, "256"),
+                                         (1 << 20, 16, sb.PRECISION_SPLIT_FP32, "512"),
                                          (1 << 22, 128, sb.PRECISION_SPLIT_FP32, "512"),
                                          (1 << 22, 128, sb.PRECISION_SPLIT_FP32, "256"),
                                          (1 << 24, 256, sb.PRECISION_SPLIT_FP32, "512"),

@@ -373,4 +373,105 @@ __device__ __forceinline__ void tile_fft_rows(V *sm, const V *__restrict__ tw, c
   }
 }
 
+// tile_fft_rows for FP32 tasks of C = 4 rows with each thread on a pair of
+// rows (2*cp, 2*cp + 1): every twiddle, and in the epilogue every
+// ph(M1*k2) and amplitude pair, is loaded once for both rows, and the two
+// outputs of a position leave as one 16-byte store.  First and middle stages:
+// a half-warp is 2 pairs x 8 consecutive butterflies, rows 2*cp at 8-byte
+// slots 0 / 8 of a 128-byte group (PR = 4 mod 16) and rows 2*cp + 1 at 4 / 12,
+// so both loads of a position are conflict-free.  Last stage: 16-byte loads
+// of position pairs (2m, 2m + 1) in the pair order m ^ (blk & 3) (a quarter-
+// warp, 2 row pairs x 4 butterflies, on 8 distinct 16-byte slots), two
+// conditional swaps restore the order.  Same arithmetic, in the same order,
+// as tile_fft_rows.
+template <typename V, int R0, int R1, int R2, int PR, int NT, class Emit>
+__device__ __forceinline__ void tile_fft_rows2(V *sm, const V *__restrict__ tw, const Emit &emit)
+{
+  constexpr int CH = 2;                                      // row pairs per task
+  constexpr int RL = (R2 > 1) ? R2 : R1;
+  constexpr int L = R0 * R1 * R2;
+  constexpr int span0 = L / R0;
+  constexpr int NP = RL / 2;                                 // position pairs of a last-stage butterfly
+  static_assert(sizeof(V) == 8 && RL % 8 == 0 && PR % 16 == 4, "FP32 rows, pair order over 4 pairs");
+  {
+    constexpr int n = CH * span0;
+#pragma unroll 1
+    for (int q = threadIdx.x; q < n; q += NT) {
+      const int cp = q % CH, i = q / CH;
+      V *p0 = sm + 2 * cp * PR + i;
+      V *p1 = p0 + PR;
+      V v[R0], w[R0];
+#pragma unroll
+      for (int r = 0; r < R0; ++r) { v[r] = p0[r * span0]; w[r] = p1[r * span0]; }
+      RegDFT<V, R0>::run(v);
+      RegDFT<V, R0>::run(w);
+      p0[0] = v[0];
+      p1[0] = w[0];
+#pragma unroll
+      for (int k = 1; k < R0; ++k) {
+        const V t = __ldg(tw + (k - 1) * span0 + i);
+        p0[k * span0] = cmul(v[k], t);
+        p1[k * span0] = cmul(w[k], t);
+      }
+    }
+  }
+  __syncthreads();
+  if constexpr (R2 > 1) {
+    constexpr int span1 = span0 / R1;                       // = RL
+    constexpr int n = CH * (L / R1);
+#pragma unroll 1
+    for (int q = threadIdx.x; q < n; q += NT) {
+      const int cp = q % CH, t = q / CH;
+      const int blk = t / span1, i = t - blk * span1;
+      V *p0 = sm + 2 * cp * PR + blk * span0 + i;
+      V *p1 = p0 + PR;
+      V v[R1], w[R1];
+#pragma unroll
+      for (int r = 0; r < R1; ++r) { v[r] = p0[r * RL]; w[r] = p1[r * RL]; }
+      RegDFT<V, R1>::run(v);
+      RegDFT<V, R1>::run(w);
+      p0[0] = v[0];
+      p1[0] = w[0];
+#pragma unroll
+      for (int k = 1; k < R1; ++k) {
+        const V t = __ldg(tw + (R0 - 1) * span0 + (k - 1) * span1 + i);
+        p0[k * RL] = cmul(v[k], t);
+        p1[k * RL] = cmul(w[k], t);
+      }
+    }
+    __syncthreads();
+  }
+  {
+    constexpr int n = CH * (L / RL);
+#pragma unroll 1
+    for (int q = threadIdx.x; q < n; q += NT) {
+      const int cp = q % CH, blk = q / CH;
+      const float4 *p0 = reinterpret_cast<const float4 *>(sm + 2 * cp * PR + blk * RL);
+      const float4 *p1 = reinterpret_cast<const float4 *>(sm + (2 * cp + 1) * PR + blk * RL);
+      int fbase;
+      if constexpr (R2 > 1) fbase = (blk / R1) + R0 * (blk % R1);
+      else fbase = blk;
+      const int x = blk & 3;
+      float4 a[NP], b[NP], c[NP], d[NP];
+#pragma unroll
+      for (int m = 0; m < NP; ++m) { a[m] = p0[m ^ x]; c[m] = p1[m ^ x]; }
+#pragma unroll
+      for (int m = 0; m < NP; ++m) { b[m] = (x & 1) ? a[m ^ 1] : a[m]; d[m] = (x & 1) ? c[m ^ 1] : c[m]; }
+#pragma unroll
+      for (int m = 0; m < NP; ++m) { a[m] = (x & 2) ? b[m ^ 2] : b[m]; c[m] = (x & 2) ? d[m ^ 2] : d[m]; }
+      V v[RL], w[RL];
+#pragma unroll
+      for (int m = 0; m < NP; ++m) {
+        v[2 * m] = cmk<V>(a[m].x, a[m].y);
+        v[2 * m + 1] = cmk<V>(a[m].z, a[m].w);
+        w[2 * m] = cmk<V>(c[m].x, c[m].y);
+        w[2 * m + 1] = cmk<V>(c[m].z, c[m].w);
+      }
+      RegDFT<V, RL>::run(v);
+      RegDFT<V, RL>::run(w);
+      emit.template run2<RL>(cp, fbase, L / RL, v, w, blk);
+    }
+  }
+}
+
 }  // namespace soi

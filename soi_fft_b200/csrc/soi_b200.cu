@@ -69,6 +69,7 @@ struct Plan {
   int discard = 1;             // drop consumed intermediate lines from L2
   int amp_keep = 0;            // demodulation amplitude loads hint L2 evict_last
   int bulk2 = 0;               // pass-2 rows by bulk copies
+  int rows2 = 0;               // FP32 pass-2 threads on row pairs
   int wait_extra = 0;          // failure test: pass-2 waits for a count that never comes
   void *d_amp = nullptr;            // [M1][M2] real demodulation amplitude, pass-2 store order
   void *d_ctw1 = nullptr, *d_ctw2 = nullptr;   // tile-FFT twiddles of the two passes, warp read order
@@ -542,6 +543,11 @@ int setup_s2ct(Plan &p, int idx)
   // 6.69 vs 7.01 ms at N = 2^28, S = 64 (FP64), bit-identical output;
   // SOI_STAGE2_BULK2=0 selects cp.async
   p.bulk2 = env_int("SOI_STAGE2_BULK2", 1) ? 1 : 0;
+  // FP32 pass 2 with each thread on a pair of rows (tile_fft_rows2): the
+  // twiddles, ph(M1*k2) and amplitude pairs loaded once for both rows, one
+  // 16-byte store per output pair: 5.43 vs 5.63 ms at N = 2^29, S = 128;
+  // SOI_STAGE2_ROWS2=0 selects one row per thread
+  p.rows2 = env_int("SOI_STAGE2_ROWS2", 1) ? 1 : 0;
   // failure-detection test only: every pass-2 task then waits for one more
   // pass-1 completion than exists, runs out its iteration limit and the
   // compute returns SOI_ERR_TIMEOUT
@@ -562,6 +568,7 @@ int launch_s2ct(Plan &p, const Exec &ex)
   a.tail = p.f2_tail;
   a.amp_keep = p.amp_keep;
   a.bulk2 = p.bulk2;
+  a.rows2 = p.rows2;
   a.err = (int *)ex.sync; a.counter = ex.sync + 1; a.done1 = ex.sync + 2;
   // counters restart; the error flag stays set until the owner clears it
   CK(cudaMemsetAsync(ex.sync + 1, 0, (size_t)(a.S + 1) * sizeof(unsigned int), ex.st));

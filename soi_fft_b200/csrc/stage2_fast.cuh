@@ -108,6 +108,7 @@ struct S2ArgsCT {
   int tail;                   // pass-2 tasks that end a block after its interleaved part (0 .. M1/C)
   int amp_keep;               // 1: amp loads carry an L2 evict_last hint
   int bulk2;                  // 1: pass-2 rows arrive by bulk copies
+  int rows2;                  // 1: FP32 pass-2 threads on row pairs (tile_fft_rows2)
   unsigned int *counter, *done1;
   int *err;
 };
@@ -202,6 +203,39 @@ template <typename V, int M1, int M2, int C, int RL, bool BATCH> struct EmitRows
         const int k = k1 + M1 * (fbase + fstep * j);
         const V w = cscale(cmul(p1, __ldg(ph2 + pos)), (a->amp_keep ? ldg_hint(amp + pos * C, pol) : __ldg(amp + pos * C)));
         if (k < M) stcs(oseg + k, cmul(v[j], w));
+      }
+    }
+  }
+};
+
+// EmitRowsCT for a pair of rows (2*cp, 2*cp + 1) of an FP32 task of C = 4
+// rows: ph(M1*k2) and the two rows' amplitudes (adjacent in the table) are
+// loaded once per position, and outputs k and k + 1 (k even, so both or
+// neither below M) leave as one 16-byte streaming store.  The same products,
+// in the same order, as EmitRowsCT.
+template <int M1, int M2, int RL> struct EmitRowsCT2 {
+  float2 *oseg; int k1_0; const float2 *ph1; const S2ArgsCT *a;
+  template <int RLx> __device__ __forceinline__ void run2(int cp, int fbase, int fstep, const float2 *v,
+                                                          const float2 *w, int blk) const
+  {
+    static_assert(RLx == RL, "last radix");
+    constexpr int C = 4;
+    const int ka = k1_0 + 2 * cp;
+    const int M = a->M;
+    const float2 pa = ph1[2 * cp], pb = ph1[2 * cp + 1];
+    const float2 *ph2 = reinterpret_cast<const float2 *>(a->ph2);
+    const float2 *amp = reinterpret_cast<const float2 *>(reinterpret_cast<const float *>(a->amp) +
+                                                        (size_t)k1_0 * M2 + 2 * cp);
+#pragma unroll
+    for (int j = 0; j < RL; ++j) {
+      const int pos = blk + fstep * j;
+      const float2 ph = __ldg(ph2 + pos);
+      const float2 am = __ldg(amp + pos * (C / 2));
+      const float2 wa = cscale(cmul(pa, ph), am.x), wb = cscale(cmul(pb, ph), am.y);
+      const int k = ka + M1 * (fbase + fstep * j);
+      if (k < M) {
+        const float2 ya = cmul(v[j], wa), yb = cmul(w[j], wb);
+        __stcs(reinterpret_cast<float4 *>(oseg + k), make_float4(ya.x, ya.y, yb.x, yb.y));
       }
     }
   }
@@ -424,7 +458,19 @@ __global__ void __launch_bounds__(NT, MINB) k_stage2_ct(S2ArgsCT a, const __grid
       }
       EmitRowsCT<V, M1, M2, C, RLB, (MINB <= 2)> e{ reinterpret_cast<V *>(a.out) + (size_t)(a.seg_lo + seg) * a.M, k1_0, s_tab, &a,
                                                     amp_pol };
-      if constexpr (G::BULK2) tile_fft_rows<V, B0, B1, B2, C, G::PR2, NT>(buf, reinterpret_cast<const V *>(a.tw2), e);
+      if constexpr (G::BULK2) {
+        if constexpr (G::E == 8 && C == 4) {
+          if (a.rows2) {
+            EmitRowsCT2<M1, M2, RLB> e2{ reinterpret_cast<float2 *>(a.out) + (size_t)(a.seg_lo + seg) * a.M, k1_0,
+                                         reinterpret_cast<const float2 *>(s_tab), &a };
+            tile_fft_rows2<V, B0, B1, B2, G::PR2, NT>(buf, reinterpret_cast<const V *>(a.tw2), e2);
+          } else {
+            tile_fft_rows<V, B0, B1, B2, C, G::PR2, NT>(buf, reinterpret_cast<const V *>(a.tw2), e);
+          }
+        } else {
+          tile_fft_rows<V, B0, B1, B2, C, G::PR2, NT>(buf, reinterpret_cast<const V *>(a.tw2), e);
+        }
+      }
       if (tid == 0) take(slot ^ 1);                           // after thread 0's own stores
     } else {
       const int k1_0 = tile * C;

@@ -257,10 +257,12 @@ def test_bulk_copy_staging_equals_cp_async_staging(N, S, prec, nt, monkeypatch):
 def test_tensor_copy_staging_equals_cp_async_staging(N, S, prec, band, monkeypatch):
     # the persistent stage 2 stages pass-1 tiles by tensor copies (a swizzled
     # dense tile) or by cp.async (a padded tile): the same arithmetic on the
-    # same values, so the outputs are identical
+    # same values, so the outputs are identical (pass 2 with one row per
+    # thread in both; its row-pair threads are compared to rounding elsewhere)
     x = _input(N, prec)
     lo, hi = (0, S) if band == "all" else band
     outs = []
+    monkeypatch.setenv("SOI_STAGE2_ROWS2", "0")
     for tma in ("1", "0"):
         monkeypatch.setenv("SOI_STAGE2_TMA", tma)
         d = _desc(N, S, prec)
@@ -311,6 +313,7 @@ def test_bulk_copied_pass2_rows_equal_cp_async_rows(N, S, prec, band, monkeypatc
     outs = []
     for bulk in ("1", "0"):
         monkeypatch.setenv("SOI_STAGE2_BULK2", bulk)
+        monkeypatch.setenv("SOI_STAGE2_ROWS2", "0")
         d = _desc(N, S, prec)
         try:
             y = torch.zeros_like(x)
@@ -320,3 +323,34 @@ def test_bulk_copied_pass2_rows_equal_cp_async_rows(N, S, prec, band, monkeypatc
         finally:
             d.free()
     assert torch.equal(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("N,S", [(1 << 20, 16), (1 << 22, 32), (1 << 27, 32)])
+@pytest.mark.parametrize("band", ["all", (3, 7)])
+def test_row_pair_pass2_agrees_with_single_rows(N, S, band, monkeypatch):
+    # FP32 pass 2 with each thread on a pair of rows (tile_fft_rows2) against
+    # one row per thread: the same products, whose fused multiply-adds the
+    # compiler may pair differently, so the outputs agree to rounding (the
+    # split form's own error against the exact DFT is ~3.6e-7), and both meet
+    # the split tolerance against the FP64 oracle
+    prec = sb.PRECISION_SPLIT_FP32
+    x = _input(N, prec)
+    lo, hi = (0, S) if band == "all" else band
+    outs = []
+    for rows2 in ("0", "1"):
+        monkeypatch.setenv("SOI_STAGE2_ROWS2", rows2)
+        d = _desc(N, S, prec)
+        try:
+            y = torch.zeros_like(x)
+            d.compute_segments(x, y, lo, hi)
+            torch.cuda.synchronize()
+            outs.append(y.to(torch.complex128))
+        finally:
+            d.free()
+    M = N // S
+    a, b = outs[0][lo * M:hi * M], outs[1][lo * M:hi * M]
+    assert float(torch.linalg.norm(a - b) / torch.linalg.norm(a)) <= 5e-7
+    assert torch.equal(outs[0][:lo * M], outs[1][:lo * M]) and torch.equal(outs[0][hi * M:], outs[1][hi * M:])
+    X = torch.fft.fft(x.to(torch.complex128))[lo * M:hi * M]
+    for y in (a, b):
+        assert float(torch.linalg.norm(y - X) / torch.linalg.norm(X)) <= 1e-6

@@ -145,3 +145,25 @@ def test_plan_variant_picks_the_measured_defaults(monkeypatch):
     assert sb.plan_variant(1 << 29, 128, sb.PRECISION_SPLIT_FP32)["stage1_threads"] == 256
     monkeypatch.setenv("SOI_STAGE2_BULK2", "0")
     assert sb.plan_variant(1 << 29, 128, sb.PRECISION_SPLIT_FP32)["pass2_staging"] == "cp.async"
+
+
+@pytest.mark.parametrize("N,S,prec", [(1 << 20, 16, sb.PRECISION_SPLIT_FP32), (1 << 26, 16, sb.PRECISION_SPLIT_FP32),
+                                      (1 << 22, 8, sb.PRECISION_FP64), (1 << 29, 128, sb.PRECISION_SPLIT_FP32),
+                                      (1 << 24, 256, sb.PRECISION_SPLIT_FP32)])
+@pytest.mark.parametrize("nt", ["256", "512"])
+def test_tensor_copy_tiles_fit_one_box(N, S, prec, nt, monkeypatch):
+    # a stage-1 phase's rows travel as one tensor-copy box of at most 256
+    # rows of at most 256 eight-byte values: the plan keeps JT + B/d - 1
+    # within it whenever it stages by tensor copies
+    monkeypatch.setenv("SOI_STAGE1_NT", nt)
+    v = sb.plan_variant(N, S, prec)
+    g = sb.plan_geometry(N, S, prec)
+    if v["stage1_staging"] == "tensor copies":
+        elem = 8 if prec == sb.PRECISION_SPLIT_FP32 else 16
+        assert g["JT"] + g["taps_per_phase"] - 1 <= 256
+        assert S * elem // 8 <= 256 and S * elem >= 128
+
+
+def test_sixty_four_byte_rows_stage_by_cp_async():
+    assert sb.plan_variant(1 << 20, 8, sb.PRECISION_SPLIT_FP32)["stage1_staging"] == "cp.async"
+    assert sb.plan_variant(1 << 20, 8, sb.PRECISION_FP64)["stage1_staging"] == "tensor copies"

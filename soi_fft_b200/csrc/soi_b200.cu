@@ -568,7 +568,9 @@ int launch_s2ct(Plan &p, const Exec &ex)
   a.tail = p.f2_tail;
   a.amp_keep = p.amp_keep;
   a.bulk2 = p.bulk2;
-  a.rows2 = p.rows2;
+  // row pairs store outputs k, k + 1 (k even) as one 16-byte store: M even
+  // and the output 16-byte aligned, else one row per thread
+  a.rows2 = p.rows2 && p.M % 2 == 0 && p.M1 % 2 == 0 && ((uintptr_t)ex.out & 15) == 0 ? 1 : 0;
   a.err = (int *)ex.sync; a.counter = ex.sync + 1; a.done1 = ex.sync + 2;
   // counters restart; the error flag stays set until the owner clears it
   CK(cudaMemsetAsync(ex.sync + 1, 0, (size_t)(a.S + 1) * sizeof(unsigned int), ex.st));

@@ -354,3 +354,25 @@ def test_row_pair_pass2_agrees_with_single_rows(N, S, band, monkeypatch):
     X = torch.fft.fft(x.to(torch.complex128))[lo * M:hi * M]
     for y in (a, b):
         assert float(torch.linalg.norm(y - X) / torch.linalg.norm(X)) <= 1e-6
+
+
+def test_output_aligned_to_eight_bytes_only_is_written_by_single_rows():
+    # pass-2 row pairs store 16 bytes at a time; an output view aligned to 8
+    # bytes only takes the one-row-per-thread stores (results equal to
+    # rounding, both within the split tolerance)
+    N, S, prec = 1 << 22, 32, sb.PRECISION_SPLIT_FP32
+    x = _input(N, prec)
+    d = _desc(N, S, prec)
+    try:
+        y = torch.empty_like(x)
+        d.compute_into(x, y)
+        big = torch.zeros(N + 1, dtype=torch.complex64, device="cuda")
+        y8 = big[1:]
+        d.compute_into(x, y8)
+        torch.cuda.synchronize()
+        a, b = y.to(torch.complex128), y8.to(torch.complex128)
+        assert float(torch.linalg.norm(a - b) / torch.linalg.norm(a)) <= 5e-7
+        X = torch.fft.fft(x.to(torch.complex128))
+        assert float(torch.linalg.norm(b - X) / torch.linalg.norm(X)) <= 1e-6
+    finally:
+        d.free()

@@ -1060,24 +1060,29 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 // laid out over the whole swizzle span, which the dense tile has no room
 // for.)  The encoder checks base, strides and box against the hardware's
 // rules; if it refuses, the kernel stages pass-1 tiles with cp.async.
-void make_pass1_map(Plan &p)
+// The pass-1 tensor map of a persistent stage-2 plan over the T buffer `T`
+// (the plan's own, or a batch chain's); false where the plan stages pass 1
+// with cp.async.  Measured against cp.async staging: 6.09 vs 6.36 ms at
+// N = 2^29 (split), 0.99 vs 1.00 ms at 2^26, 8.09 vs 8.33 ms at 2^28 in FP64;
+// SOI_STAGE2_TMA=0 selects cp.async (tests compare the two).
+bool pass1_map(const Plan &p, void *T, CUtensorMap *map)
 {
-  p.tma1 = false;
-  // measured against cp.async staging: 6.09 vs 6.36 ms at N = 2^29 (split),
-  // 0.99 vs 1.00 ms at 2^26, 8.09 vs 8.33 ms at 2^28 in FP64;
-  // SOI_STAGE2_TMA=0 selects cp.async (tests compare the two)
-  if (p.fast2 != 3 || !p.d_T || p.f2_boxr <= 0 || !env_int("SOI_STAGE2_TMA", 1)) return;
+  if (p.fast2 != 3 || !T || p.f2_boxr <= 0 || !env_int("SOI_STAGE2_TMA", 1)) return false;
   const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
-  if (!enc) return;
+  if (!enc) return false;
   const bool f64 = p.prec == SOI_PRECISION_FP64;
   const cuuint64_t dims[2] = { (cuuint64_t)2 * p.M2, (cuuint64_t)p.S * p.M1 };
   const cuuint64_t strides[1] = { (cuuint64_t)p.M2 * p.elem };
   const cuuint32_t box[2] = { (cuuint32_t)(32 / (f64 ? 8 : 4)), (cuuint32_t)p.f2_boxr };
   const cuuint32_t estr[2] = { 1, 1 };
-  const CUresult r = enc(&p.tmap1, f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, p.d_T,
-                         dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                         CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  p.tma1 = r == CUDA_SUCCESS;
+  return enc(map, f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, T, dims, strides, box,
+             estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+void make_pass1_map(Plan &p)
+{
+  p.tma1 = pass1_map(p, p.d_T, &p.tmap1);
 }
 
 int make_plan(const soi_desc_t *d, size_t k, int knob_s1_nt, int knob_s2, bool with_stream, Plan **out,
@@ -1329,7 +1334,12 @@ void batch_free(Batch *b)
 int batch_enqueue(Batch &b, const BatchItem &it)
 {
   Plan &p = *b.plans[it.plan];
-  const Exec ex{ it.in, b.T[it.chain], it.out, b.sync[it.chain], it.lo, it.hi, b.streams[it.chain] };
+  // pass-1 tiles by tensor copies over this chain's T (the launch copies the
+  // map into the kernel's parameters, so a local map outlives its use)
+  CUtensorMap map;
+  const bool tma = pass1_map(p, b.T[it.chain], &map);
+  const Exec ex{ it.in, b.T[it.chain], it.out, b.sync[it.chain], it.lo, it.hi, b.streams[it.chain],
+                 tma ? &map : nullptr };
   int rc;
   if ((rc = run_stage1(p, ex))) return rc;
   if (b.tmpl.use_vlc && (rc = run_vlc(p, ex))) return rc;
@@ -1340,7 +1350,9 @@ int batch_enqueue(Batch &b, const BatchItem &it)
 int batch_time_variant(Batch &b, Plan &p, const BatchItem &it, void *out, float *ms)
 {
   cudaStream_t st = b.streams[0];
-  const Exec ex{ it.in, b.T[0], out, b.sync[0], it.lo, it.hi, st };
+  CUtensorMap map;
+  const bool tma = pass1_map(p, b.T[0], &map);
+  const Exec ex{ it.in, b.T[0], out, b.sync[0], it.lo, it.hi, st, tma ? &map : nullptr };
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));

@@ -74,7 +74,7 @@ KERNELS = {
 FP64_PROFILE = {
     "stage1": {"fp64_pipe_frac": 0.565, "traffic_ratio": 2.369 / 2.416,
                "profile": "ncu --set full at N=2^26, S=64, same instance"},
-    "stage2": {"fp64_pipe_frac": 0.242, "traffic_ratio": 5.797 / 2.416,
+    "stage2": {"fp64_pipe_frac": 0.245, "traffic_ratio": 5.790 / 2.416,
                "profile": "ncu --set full at N=2^26, S=16, same M' tiles"},
 }
 

@@ -654,12 +654,6 @@ int launch_conv_tS(Plan &p, const Exec &ex)
   CUtensorMap rmap;
   memset(&rmap, 0, sizeof rmap);
   if (BULK) a.tma_rows = input_rows_map(p, ex.in, &rmap) ? 1 : 0;
-  // tensor-copy staging needs no barrier before a phase (every thread waits
-  // on the phase's mbarrier) and, with warps releasing buffers on mbarriers,
-  // none after it: stage 1 at N = 2^29, S = 128 5.69 -> 5.42 ms, FP64 at
-  // 2^28, S = 64 5.66 -> 5.40 ms (same box), bit-identical;
-  // SOI_STAGE1_RELAX=0 keeps both barriers, 1 only the one after
-  a.relax = BULK ? env_int("SOI_STAGE1_RELAX", 2) : 0;
   auto kern = k_conv_sfft_tS<R, NMU, JR, R0, R1, NT, BULK>;
   CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem1b));
   dim3 grid((unsigned)((p.J + p.JT2 - 1) / p.JT2));

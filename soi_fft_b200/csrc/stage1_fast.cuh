@@ -32,8 +32,6 @@ struct Conv2Args {
   int seg_lo, seg_hi;    // segments sigma stored (all: 0, S)
   int *err;              // set to 1 when a staging wait gives up (bulk copies)
   int tma_rows = 0;      // the kernel's tensor map describes alpha (bulk staging)
-  int relax = 0;         // bulk staging: 1 no barrier before a phase (each thread waits on the
-                         // mbarrier), 2 also none after it (warps release buffers on mbarriers)
 };
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
@@ -232,10 +230,6 @@ template <typename V> struct EmitTransposed {
 // .cpp:495-515) takes its rows by one bulk copy per row from warp 0 instead.
 // The buffers start on 128-byte boundaries (the tensor copy's destination
 // rule), and the filter slice sits after JT + AC - 1 rows in every phase.
-// With bulk staging no CTA barrier separates the phases (a.relax = 2): each
-// thread waits on the phase's mbarrier for its data, and each warp arrives
-// on the buffer's "empty" mbarrier when done with it, which warp 0 waits on
-// (bounded) before refilling the buffer.
 // Otherwise every thread issues 16-byte cp.async.
 template <typename R, int NMU, int JR, int R0, int R1, int NT, bool BULK>
 __global__ void __launch_bounds__(NT, 512 / NT) k_conv_sfft_tS(Conv2Args a, const __grid_constant__ CUtensorMap rmap)
@@ -297,7 +291,6 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_conv_sfft_tS(Conv2Args a, cons
     for (int c = tid; c < fchunks; c += NT, fs += NT * 16, fd += NT * 16) cp_async16(fd, fs);
   };
   __shared__ unsigned long long s_mbar[2];
-  __shared__ unsigned long long s_empty[2];             // relax = 2: every warp arrives when done with a buffer
   // the same phase as bulk copies issued by warp 0 onto the buffer's mbarrier
   // rows of the box: JT + AC - 1 (the phase with fewer taps uses a prefix);
   // a tile takes the tensor copy when every phase's box ends inside [0, J)
@@ -344,30 +337,14 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_conv_sfft_tS(Conv2Args a, cons
       }
     }
   };
-  const int relax = BULK ? a.relax : 0;
   if (BULK) {
     if (tid == 0) {
       mbar_init(&s_mbar[0], 1);
       mbar_init(&s_mbar[1], 1);
-      mbar_init(&s_empty[0], NT / 32);
-      mbar_init(&s_empty[1], NT / 32);
       mbar_init_fence();
     }
     __syncthreads();
   }
-  // relax = 2: warp 0 waits until every warp has released buffer b (the
-  // k-th release of b completes phase k of s_empty[b]) before refilling it;
-  // bounded, a wait that gives up flags the error and refills anyway (the
-  // transform is then reported failed, its values are not used)
-  auto wait_empty = [&](int b, unsigned parity) {
-    if (tid == 0) {
-      long long it = 0;
-      while (!mbar_try_wait(&s_empty[b], parity)) {
-        if (++it > kBulkWaitLimit) { atomicExch(a.err, 1); break; }
-      }
-    }
-    __syncwarp();
-  };
 
   V acc[JR][NMU];
 #pragma unroll
@@ -384,11 +361,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_conv_sfft_tS(Conv2Args a, cons
   for (int p = 0; p < nphase; ++p) {
     V *cur = (p & 1) ? buf1 : buf0;
     if (BULK) {
-      if (p + 1 < nphase) {
-        // buffer (p + 1) & 1 last held phase p - 1
-        if (relax == 2 && p >= 1 && tid < 32) wait_empty((p + 1) & 1, (unsigned)(((p - 1) >> 1) & 1));
-        issue_bulk(p + 1, (p & 1) ? buf0 : buf1, &s_mbar[(p + 1) & 1]);
-      }
+      if (p + 1 < nphase) issue_bulk(p + 1, (p & 1) ? buf0 : buf1, &s_mbar[(p + 1) & 1]);
       wait_bulk(p);
     } else if (p + 1 < nphase) {
       issue(p + 1, (p & 1) ? buf0 : buf1);
@@ -397,7 +370,10 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_conv_sfft_tS(Conv2Args a, cons
     } else {
       cp_async_wait<0>();
     }
-    if (relax == 0) __syncthreads();                        // (bulk: each thread has waited on the mbarrier)
+    // cp.async: the barrier makes every thread's copies visible to all; bulk
+    // staging needs none here, every thread has waited on the phase's
+    // mbarrier, which makes the copy's bytes visible to it
+    if (!BULK) __syncthreads();
     if (active) {
       const int a_lo = (p % nch) * a.AC;
       const int n_a = min(a.AC, a.atap - a_lo);
@@ -439,14 +415,8 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_conv_sfft_tS(Conv2Args a, cons
         }
       }
     }
-    if (relax == 2) {
-      __syncwarp();
-      if ((tid & 31) == 0) mbar_arrive(&s_empty[p & 1]);   // this warp is done with buffer p & 1
-    } else {
-      __syncthreads();
-    }
+    __syncthreads();
   }
-  if (relax == 2) __syncthreads();                          // every warp is done with the buffers the tile reuses
   if (active) {
     const V *ph = reinterpret_cast<const V *>(a.phase);
 #pragma unroll

@@ -237,9 +237,8 @@ def test_bulk_copy_staging_equals_cp_async_staging(N, S, prec, nt, monkeypatch):
     x = _input(N, prec)
     outs = []
     monkeypatch.setenv("SOI_STAGE1_NT", nt)
-    for bulk, relax in (("0", "0"), ("1", "0"), ("1", "1"), ("1", "2")):
+    for bulk in ("0", "1"):
         monkeypatch.setenv("SOI_STAGE1_BULK", bulk)
-        monkeypatch.setenv("SOI_STAGE1_RELAX", relax)
         d = _desc(N, S, prec)
         try:
             y = torch.empty_like(x)
@@ -248,7 +247,7 @@ def test_bulk_copy_staging_equals_cp_async_staging(N, S, prec, nt, monkeypatch):
             outs.append(y)
         finally:
             d.free()
-    assert all(torch.equal(outs[0], o) for o in outs[1:])
+    assert torch.equal(outs[0], outs[1])
 
 
 @pytest.mark.parametrize("N,S,prec", [(1 << 20, 16, sb.PRECISION_SPLIT_FP32), (1 << 22, 32, sb.PRECISION_SPLIT_FP32),

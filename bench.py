@@ -60,7 +60,7 @@ CPU_SAMPLE_LOG2N = 26
 # N = 2^28, S = 64, the same M' = 2560 x 2048 tiles as N = 2^29, S = 128 (its
 # L2 residency depends on the segment size, so a smaller M' would not carry).
 KERNELS = {
-    "stage1": ("k_conv_sfft_tS (stage 1: convolution + S-point FFTs + transposed store)", 1160.6 / 1208.0,
+    "stage1": ("k_conv_sfft_tS (stage 1: convolution + S-point FFTs + transposed store)", 1160.1 / 1208.0,
                "ncu at N=2^26, S=128 (same kernel instance), scaled by the units processed"),
     "stage2": ("k_stage2_ct (stage 2: M'-point four-step FFT + demodulation + discard)", 4378.3 / 2415.9,
                "ncu at N=2^27, S=32 (same M' tiles), scaled by the segments"),
